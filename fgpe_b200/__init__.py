@@ -1,0 +1,277 @@
+"""fgpe_b200 -- B200-native Gross-Pitaevskii solver (Python side of the C ABI).
+
+The product is ``libgpe.so`` (hand-written sm_100a CUDA kernels behind the C
+ABI of ``include/gpe.h``) plus the ``gpe`` command-line driver.  This module is
+a thin ctypes mirror of that ABI for tests, the benchmark and Python users; it
+loads the in-tree library and fails loudly when it is missing -- there is no
+CPU fallback.
+
+Grid arrays are numpy complex128 of shape (nz, ny, nx) (x fastest, the
+reference's index z*NX*NY + y*NX + x, hpp/header.hpp:20).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, byref, c_double, c_int, c_longlong, c_void_p
+
+import numpy as np
+
+__all__ = [
+    "GPEConfig", "GPEError", "Solver", "lib", "make_config", "grid_axes",
+    "C128", "C64", "HAM_BEC", "HAM_BEC2", "HAM_TEMPLATE", "HAM_DIPOLAR",
+    "IMAG_HEAVYBALL", "IMAG_RK4", "NO_HAMIL_PARAMS",
+]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgpe.so")
+
+NO_HAMIL_PARAMS = 32
+C128, C64 = 0, 1
+HAM_BEC, HAM_BEC2, HAM_TEMPLATE, HAM_DIPOLAR = 0, 1, 2, 3
+IMAG_HEAVYBALL, IMAG_RK4 = 0, 1
+ABI_VERSION = 1
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported", 3: "CUDA error",
+          4: "out of memory", 5: "diverged", 6: "timeout", 7: "I/O error"}
+
+
+class GPEError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"gpe status {status} ({STATUS.get(status, '?')}): {msg}")
+        self.status = status
+
+
+class GPEConfig(ctypes.Structure):
+    """ctypes image of ``gpe_config`` (include/gpe.h)."""
+    _fields_ = [
+        ("abi_version", c_int), ("nx", c_int), ("ny", c_int), ("nz", c_int), ("dim", c_int),
+        ("xmax", c_double * 3), ("dx", c_double * 3),
+        ("ncomp", c_int), ("precision", c_int), ("hamiltonian", c_int), ("imag_scheme", c_int),
+        ("prms", c_double * NO_HAMIL_PARAMS), ("dt", c_double), ("beta", c_double),
+        ("npart", c_double * 2), ("epsilon_e", c_double), ("reserved", c_int * 8),
+    ]
+
+    def copy(self) -> "GPEConfig":
+        c = GPEConfig()
+        ctypes.memmove(byref(c), byref(self), ctypes.sizeof(GPEConfig))
+        return c
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libgpe.so from the package directory (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} not found: build it with `make -C fgpe_b200` "
+                           "(or __graft_entry__.build()); there is no CPU fallback")
+    L = ctypes.CDLL(LIB_PATH)
+    H = c_void_p
+    P = POINTER(c_double)
+    sig = {
+        "gpe_abi_version": (c_int, []),
+        "gpe_last_error_string": (ctypes.c_char_p, []),
+        "gpe_status_string": (ctypes.c_char_p, [c_int]),
+        "gpe_config_init": (c_int, [POINTER(GPEConfig)]),
+        "gpe_fft_length_supported": (c_int, [c_int]),
+        "gpe_create": (c_int, [POINTER(GPEConfig), POINTER(H)]),
+        "gpe_destroy": (c_int, [H]),
+        "gpe_set_stream": (c_int, [H, c_void_p]),
+        "gpe_set_params": (c_int, [H, P]),
+        "gpe_set_psi": (c_int, [H, c_int, P]),
+        "gpe_get_psi": (c_int, [H, c_int, P]),
+        "gpe_set_vext": (c_int, [H, c_int, P]),
+        "gpe_set_psi_device": (c_int, [H, c_int, c_void_p]),
+        "gpe_get_psi_device": (c_int, [H, c_int, c_void_p]),
+        "gpe_step_real": (c_int, [H, c_int, c_int, P]),
+        "gpe_step_imag": (c_int, [H, c_int, c_int, POINTER(c_int), POINTER(c_int)]),
+        "gpe_imag_state": (c_int, [H, P]),
+        "gpe_reset_imag_state": (c_int, [H]),
+        "gpe_laplace": (c_int, [H, c_int, P]),
+        "gpe_apply_h": (c_int, [H, c_double, c_int, P, P]),
+        "gpe_observables": (c_int, [H, c_double, P]),
+        "gpe_fft": (c_int, [H, c_int, c_int]),
+        "gpe_sync": (c_int, [H]),
+        "gpe_kernel_launches": (c_longlong, [H]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    if L.gpe_abi_version() != ABI_VERSION:
+        raise RuntimeError("libgpe ABI version mismatch")
+    _lib = L
+    return L
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        msg = lib().gpe_last_error_string()
+        raise GPEError(status, msg.decode() if msg else "")
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(POINTER(c_double))
+
+
+def grid_axes(cfg: GPEConfig):
+    """Cell-centred x, y, z axes (src/baseHamiltonian.cu:25-51)."""
+    out = []
+    for d, n in enumerate((cfg.nx, cfg.ny, cfg.nz)):
+        zero = (cfg.dim == 1 and d > 0) or (cfg.dim == 2 and d == 2)
+        i = np.arange(n, dtype=np.float64)
+        out.append(np.zeros(n) if zero else -cfg.xmax[d] + i * cfg.dx[d] + 0.5 * cfg.dx[d])
+    return out
+
+
+def make_config(shape, xmax, *, dt=1e-3, ncomp=1, precision=C128, hamiltonian=HAM_BEC,
+                imag_scheme=IMAG_HEAVYBALL, g=0.0, prms=None, beta=0.0, npart=(1.0, 1.0),
+                epsilon_e=0.0, dim=None) -> GPEConfig:
+    """Config in code units.  shape = (nx, ny, nz); xmax = half box widths.
+
+    ``g`` sets a constant contact coupling g = 4 pi a for the BEC plugin
+    (d_h_params = {a, a, a, 0, 0, 0}); ``prms`` overrides d_h_params entirely.
+    """
+    c = GPEConfig()  # zero-initialised, as gpe_config_init does
+    c.abi_version = ABI_VERSION
+    nx, ny, nz = shape
+    c.nx, c.ny, c.nz = nx, ny, nz
+    if dim is None:
+        dim = 3 if nz > 1 else (2 if ny > 1 else 1)
+    c.dim = dim
+    xm = list(xmax) if np.ndim(xmax) else [xmax] * 3
+    for d in range(3):
+        c.xmax[d] = xm[d]
+        c.dx[d] = 2.0 * xm[d] / (nx, ny, nz)[d]
+    c.ncomp = ncomp
+    c.precision = precision
+    c.hamiltonian = hamiltonian
+    c.imag_scheme = imag_scheme
+    if prms is None:
+        prms = np.zeros(NO_HAMIL_PARAMS)
+        a = g / (4.0 * 3.141592653589793)
+        prms[0:3] = a
+    for i in range(NO_HAMIL_PARAMS):
+        c.prms[i] = float(prms[i]) if i < len(prms) else 0.0
+    c.dt = dt
+    c.beta = beta
+    c.npart[0], c.npart[1] = npart
+    c.epsilon_e = epsilon_e
+    return c
+
+
+class Solver:
+    """One libgpe handle (owns its device buffers)."""
+
+    def __init__(self, cfg: GPEConfig):
+        self.cfg = cfg.copy()
+        self.shape = (cfg.nz, cfg.ny, cfg.nx)
+        self.N = cfg.nx * cfg.ny * cfg.nz
+        h = c_void_p()
+        _check(lib().gpe_create(byref(self.cfg), byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gpe_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream_ptr: int) -> None:
+        _check(lib().gpe_set_stream(self._h, c_void_p(stream_ptr)))
+
+    def set_params(self, prms) -> None:
+        p = np.zeros(NO_HAMIL_PARAMS)
+        p[: len(prms)] = prms
+        _check(lib().gpe_set_params(self._h, _dp(p)))
+
+    def _c128(self, arr) -> np.ndarray:
+        a = np.ascontiguousarray(arr, dtype=np.complex128).reshape(-1)
+        if a.size != self.N:
+            raise ValueError(f"expected {self.N} points, got {a.size}")
+        return a
+
+    def set_psi(self, comp: int, psi) -> None:
+        a = self._c128(psi)
+        _check(lib().gpe_set_psi(self._h, comp, _dp(a.view(np.float64))))
+
+    def get_psi(self, comp: int = 0) -> np.ndarray:
+        out = np.empty(self.N, np.complex128)
+        _check(lib().gpe_get_psi(self._h, comp, _dp(out.view(np.float64))))
+        return out.reshape(self.shape)
+
+    def set_vext(self, comp: int, v) -> None:
+        a = self._c128(v)
+        _check(lib().gpe_set_vext(self._h, comp, _dp(a.view(np.float64))))
+
+    def set_psi_device(self, comp: int, ptr: int) -> None:
+        _check(lib().gpe_set_psi_device(self._h, comp, c_void_p(ptr)))
+
+    def get_psi_device(self, comp: int, ptr: int) -> None:
+        _check(lib().gpe_get_psi_device(self._h, comp, c_void_p(ptr)))
+
+    def step_real(self, first_iteration: int, nsteps: int, want_obs: bool = False):
+        if want_obs:
+            obs = np.zeros(6)
+            _check(lib().gpe_step_real(self._h, first_iteration, nsteps, _dp(obs)))
+            return obs[: 3 * self.cfg.ncomp]
+        _check(lib().gpe_step_real(self._h, first_iteration, nsteps, None))
+        return None
+
+    def step_imag(self, first_iteration: int, nsteps: int):
+        done, conv = c_int(0), c_int(0)
+        _check(lib().gpe_step_imag(self._h, first_iteration, nsteps, byref(done), byref(conv)))
+        return done.value, bool(conv.value)
+
+    def imag_state(self) -> np.ndarray:
+        out = np.zeros(8)
+        _check(lib().gpe_imag_state(self._h, _dp(out)))
+        return out[: 4 * self.cfg.ncomp]
+
+    def reset_imag_state(self) -> None:
+        _check(lib().gpe_reset_imag_state(self._h))
+
+    def laplace(self, comp: int = 0) -> np.ndarray:
+        out = np.empty(self.N, np.complex128)
+        _check(lib().gpe_laplace(self._h, comp, _dp(out.view(np.float64))))
+        return out.reshape(self.shape)
+
+    def apply_h(self, t: float, comp: int = 0):
+        hmu = np.empty(self.N, np.complex128)
+        hen = np.empty(self.N, np.complex128)
+        _check(lib().gpe_apply_h(self._h, t, comp, _dp(hmu.view(np.float64)), _dp(hen.view(np.float64))))
+        return hmu.reshape(self.shape), hen.reshape(self.shape)
+
+    def observables(self, t: float = 0.0) -> np.ndarray:
+        out = np.zeros(6)
+        _check(lib().gpe_observables(self._h, t, _dp(out)))
+        return out[: 3 * self.cfg.ncomp]
+
+    def fft(self, comp: int, sign: int) -> None:
+        _check(lib().gpe_fft(self._h, comp, sign))
+
+    def sync(self) -> None:
+        _check(lib().gpe_sync(self._h))
+
+    @property
+    def launches(self) -> int:
+        return int(lib().gpe_kernel_launches(self._h))

@@ -1,0 +1,840 @@
+// gpe_api.cu -- C ABI of libgpe: handle lifecycle, device buffers, and the
+// host-side orchestration of the fused pass chains (see include/gpe.h).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/gpe.h"
+#include "gpe_dispatch.cuh"
+#include "gpe_sizes.h"
+
+using namespace gpe;
+
+namespace {
+
+thread_local std::string g_err;
+
+gpe_status fail(gpe_status s, const std::string& msg) {
+    g_err = msg;
+    return s;
+}
+
+#define GPE_CUDA(call)                                                                                      \
+    do {                                                                                                    \
+        cudaError_t e_ = (call);                                                                            \
+        if (e_ != cudaSuccess)                                                                              \
+            return fail(e_ == cudaErrorMemoryAllocation ? GPE_ERR_OUT_OF_MEMORY : GPE_ERR_CUDA,              \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                                \
+    } while (0)
+
+#define GPE_TRY(expr)                      \
+    do {                                   \
+        gpe_status s_ = (expr);            \
+        if (s_ != GPE_OK) return s_;       \
+    } while (0)
+
+bool length_compiled(int L) {
+#define GPE_IS(n) if (L == n) return true;
+    GPE_SIZES_p2(GPE_IS) GPE_SIZES_p3(GPE_IS) GPE_SIZES_p5(GPE_IS) GPE_SIZES_p9(GPE_IS)
+#undef GPE_IS
+    return false;
+}
+
+int plan_T(int L) { return L / make_plan(L).E; }
+
+enum StateMode { ST_CANON = 0, ST_HB = 1, ST_RKI = 2 };
+
+}  // namespace
+
+struct gpe_handle {
+    gpe_config cfg;
+    int prec = GPE_C128;
+    int nx = 1, ny = 1, nz = 1;
+    long long N = 1;
+    int ncomp = 1, dens = 0, nf = 1;
+    size_t esz = 16;
+    cudaStream_t st = 0;
+    void* A[2] = {nullptr, nullptr};
+    void* B[2] = {nullptr, nullptr};
+    void* K[2] = {nullptr, nullptr};
+    void* V[2] = {nullptr, nullptr};
+    void* W[3] = {nullptr, nullptr, nullptr};
+    void* O[4] = {nullptr, nullptr, nullptr, nullptr};
+    void* tw[3] = {nullptr, nullptr, nullptr};
+    double* kax[3] = {nullptr, nullptr, nullptr};
+    void* vdd = nullptr;
+    double* prms = nullptr;
+    DevScalars* sc = nullptr;
+    double* partials = nullptr;
+    void* stage128 = nullptr;  // complex128 staging (complex64 handles)
+    long long launches = 0;
+    int mode = ST_CANON;
+    bool hb_old_valid = true;
+};
+
+// ---- small element-wise kernels ------------------------------------------------------
+namespace {
+
+template <typename C>
+__global__ void k_from_c128(C* dst, const double2* src, long long n) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = from_d<C>(src[i]);
+}
+template <typename C>
+__global__ void k_to_c128(double2* dst, const C* src, long long n) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = to_d(src[i]);
+}
+template <typename C>
+__global__ void k_copy(C* dst, const C* src, long long n) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[i];
+}
+// Materialise psi and psi_old of a lazily renormalised state (ScalarMultiply,
+// hpp/parallel.hpp:205-212): heavy ball: A <- s_cur*buf[cur], B <- s_old*buf[1-cur];
+// RK4-imaginary: A <- s_cur*A.
+template <typename C>
+__global__ void k_canon(C* A, C* B, const DevScalars* sc, int comp, int hb, long long n) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int cur = sc->cur_slot;
+    const double sc0 = sc->scale[cur][comp], sc1 = sc->scale[1 - cur][comp];
+    if (hb) {
+        const C a = A[i], b = B[i];
+        const C p = (cur == 0) ? a : b;
+        const C o = (cur == 0) ? b : a;
+        A[i] = from_d<C>(make_double2((double)p.x * sc0, (double)p.y * sc0));
+        B[i] = from_d<C>(make_double2((double)o.x * sc1, (double)o.y * sc1));
+    } else {
+        const C a = A[i];
+        A[i] = from_d<C>(make_double2((double)a.x * sc0, (double)a.y * sc0));
+    }
+}
+__global__ void k_reset_scales(DevScalars* sc) {
+    sc->scale[0][0] = sc->scale[0][1] = sc->scale[1][0] = sc->scale[1][1] = 1.0;
+    sc->cur_slot = 0;
+}
+
+inline unsigned blocks_for(long long n, int thr) { return (unsigned)((n + thr - 1) / thr); }
+
+// Host copy of the dipolar kernel (see gpe_config docs / GPE_HAM_DIPOLAR),
+// the unused DipoleDipoleInteraction of src/parallel.cu:326-352 with a
+// spherical cut-off, divided by N for the unnormalised inverse FFT.
+void host_vdd(const gpe_config& c, const std::vector<double>* k, std::vector<double>& out) {
+    const long long N = (long long)c.nx * c.ny * c.nz;
+    out.assign(N, 0.0);
+    const double add = c.prms[6];
+    double d[3] = {c.prms[7], c.prms[8], c.prms[9]};
+    const double dn = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    if (dn > 0)
+        for (double& v : d) v /= dn;
+    const double R = c.prms[10];
+    const double pi = 3.141592653589793;
+    for (int iz = 0; iz < c.nz; ++iz)
+        for (int iy = 0; iy < c.ny; ++iy)
+            for (int ix = 0; ix < c.nx; ++ix) {
+                const long long idx = ((long long)iz * c.ny + iy) * c.nx + ix;
+                const double kx = k[0][ix], ky = k[1][iy], kz = k[2][iz];
+                const double num = kx * d[0] + ky * d[1] + kz * d[2];
+                const double den = std::sqrt(kx * kx + ky * ky + kz * kz);
+                double v = 0.0;
+                if (den >= 1e-6) {
+                    v = 12.0 * pi * add * ((num / den) * (num / den) - 1.0 / 3.0);
+                    if (R > 0) {
+                        const double q = 2.0 * pi * den * R;
+                        v *= 1.0 + 3.0 * std::cos(q) / (q * q) - 3.0 * std::sin(q) / (q * q * q);
+                    }
+                }
+                out[idx] = v / (double)N;
+            }
+}
+
+// x/k axes: BaseHamiltonian::InitializeKspace, src/baseHamiltonian.cu:53-82,
+// with DKX, KXMAX of src/params.cu:206-211 (odd-N formula kept).
+void host_kaxes(const gpe_config& c, std::vector<double>* k) {
+    const int NX[3] = {c.nx, c.ny, c.nz};
+    for (int d = 0; d < 3; ++d) {
+        const int n = NX[d];
+        const double DX = c.dx[d];
+        const double DKX = 1.0 / (n * DX);
+        const double KXMAX = 1.0 / (2.0 * DX);
+        k[d].assign(n, 0.0);
+        for (int ik = 0; ik <= n / 2 && ik < n; ++ik) k[d][ik] = (ik)*DKX;
+        for (int ik = n / 2 + 1; ik < n; ++ik) k[d][ik] = -KXMAX + (ik - (n / 2)) * DKX;
+        const bool zero = (c.dim == 1 && d > 0) || (c.dim == 2 && d == 2);
+        if (zero)
+            for (int i = 0; i < n; ++i) k[d][i] = 0.0;
+    }
+}
+
+template <typename C>
+void host_twiddles(int L, std::vector<C>& tw) {
+    tw.resize(L);
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (int m = 0; m < L; ++m) {
+        const long double a = -two_pi * (long double)m / (long double)L;
+        tw[m].x = (decltype(tw[m].x))cosl(a);
+        tw[m].y = (decltype(tw[m].y))sinl(a);
+    }
+}
+
+// ---- pass chains -------------------------------------------------------------------------
+template <typename R>
+struct Ctx {
+    typedef typename Cx<R>::T C;
+    gpe_handle* h;
+    C* A(int c) const { return (C*)h->A[c]; }
+    C* B(int c) const { return (C*)h->B[c]; }
+};
+
+template <typename R>
+PassArgs<R> base_args(gpe_handle* h) {
+    typedef typename Cx<R>::T C;
+    PassArgs<R> a;
+    std::memset(&a, 0, sizeof(a));
+    a.nx = h->nx;
+    a.ny = h->ny;
+    a.nz = h->nz;
+    a.nrows = h->ny * h->nz;
+    a.ncomp = h->ncomp;
+    a.dens = h->dens;
+    for (int f = 0; f < 3; ++f) a.w[f] = (C*)h->W[f];
+    for (int c = 0; c < 2; ++c) {
+        a.buf[0][c] = (C*)h->A[c];
+        a.buf[1][c] = (C*)h->B[c];
+        a.kacc[c] = (C*)h->K[c];
+        a.vext[c] = (const C*)h->V[c];
+        a.pin[c] = (const C*)h->A[c];
+    }
+    a.kx = h->kax[0];
+    a.ky = h->kax[1];
+    a.kz = h->kax[2];
+    a.vdd = (const R*)h->vdd;
+    a.prms = h->prms;
+    a.sc = h->sc;
+    a.partials = h->partials;
+    a.ham = h->cfg.hamiltonian;
+    a.spec = SPEC_KIN;
+    a.dt = h->cfg.dt;
+    a.beta = h->cfg.beta;
+    a.lap_scale = 19.739208802 / (double)h->N;  // src/parallel.cu:199
+    a.DV = h->cfg.dx[0] * h->cfg.dx[1] * h->cfg.dx[2];
+    a.eps = h->cfg.epsilon_e;
+    a.npart[0] = h->cfg.npart[0];
+    a.npart[1] = h->cfg.npart[1];
+    return a;
+}
+
+template <typename R>
+gpe_status launch_x(gpe_handle* h, PassArgs<R> a, int nf, int mode) {
+    a.mode = mode;
+    a.tw = (const typename Cx<R>::T*)h->tw[0];
+    cudaError_t err = cudaSuccess;
+    if (!dispatch_x(h->nx, nf, a, h->st, &err))
+        return fail(GPE_ERR_UNSUPPORTED, "no x-pass kernel for length " + std::to_string(h->nx));
+    if (err != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("x pass launch: ") + cudaGetErrorString(err));
+    h->launches++;
+    return GPE_OK;
+}
+
+template <typename R>
+gpe_status launch_s(gpe_handle* h, PassArgs<R> a, int nf, int axis, int mode) {
+    const int L = axis == 1 ? h->ny : h->nz;
+    const int T = plan_T(L);
+    int tx = h->nx < 16 ? h->nx : 16;
+    while (tx > 1 && tx * T > 512) tx /= 2;
+    a.mode = mode;
+    a.sax = axis;
+    a.tx = tx;
+    a.tw = (const typename Cx<R>::T*)h->tw[axis];
+    int nouter;
+    if (axis == 1) {
+        a.sstride = h->nx;
+        a.ostride = (long long)h->nx * h->ny;
+        nouter = h->nz;
+    } else {
+        a.sstride = (long long)h->nx * h->ny;
+        a.ostride = h->nx;
+        nouter = h->ny;
+    }
+    cudaError_t err = cudaSuccess;
+    if (!dispatch_s(L, nf, a, nouter, h->st, &err))
+        return fail(GPE_ERR_UNSUPPORTED, "no strided-pass kernel for length " + std::to_string(L));
+    if (err != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("strided pass launch: ") + cudaGetErrorString(err));
+    h->launches++;
+    return GPE_OK;
+}
+
+// Full kinetic chain: x-forward with prologue, strided forward passes, the
+// last strided axis forward * k-space * inverse, strided inverse passes,
+// x-inverse with epilogue.  a.pro / a.epi / a.stage ... are set by the caller.
+template <typename R>
+gpe_status run_chain(gpe_handle* h, const PassArgs<R>& a, int nf) {
+    int axes[2], na = 0;
+    if (h->ny > 1) axes[na++] = 1;
+    if (h->nz > 1) axes[na++] = 2;
+    if (na == 0) return launch_x<R>(h, a, nf, XM_FULL);
+    GPE_TRY(launch_x<R>(h, a, nf, XM_FWD));
+    for (int i = 0; i < na - 1; ++i) GPE_TRY(launch_s<R>(h, a, nf, axes[i], SM_FWD));
+    GPE_TRY(launch_s<R>(h, a, nf, axes[na - 1], SM_FKI));
+    for (int i = na - 2; i >= 0; --i) GPE_TRY(launch_s<R>(h, a, nf, axes[i], SM_INV));
+    return launch_x<R>(h, a, nf, XM_INV);
+}
+
+gpe_status sync_read_scalars(gpe_handle* h, DevScalars* out) {
+    GPE_CUDA(cudaMemcpyAsync(out, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->st));
+    GPE_CUDA(cudaStreamSynchronize(h->st));
+    return GPE_OK;
+}
+
+template <typename R>
+gpe_status canonicalize_t(gpe_handle* h) {
+    typedef typename Cx<R>::T C;
+    if (h->mode == ST_CANON) return GPE_OK;
+    const int thr = 256;
+    for (int c = 0; c < h->ncomp; ++c) {
+        k_canon<C><<<blocks_for(h->N, thr), thr, 0, h->st>>>((C*)h->A[c], (C*)h->B[c], h->sc, c, h->mode == ST_HB,
+                                                             h->N);
+        h->launches++;
+    }
+    k_reset_scales<<<1, 1, 0, h->st>>>(h->sc);
+    h->launches++;
+    GPE_CUDA(cudaGetLastError());
+    if (h->mode == ST_RKI) h->hb_old_valid = false;
+    h->mode = ST_CANON;
+    return GPE_OK;
+}
+
+gpe_status canonicalize(gpe_handle* h) {
+    return h->prec == GPE_C64 ? canonicalize_t<float>(h) : canonicalize_t<double>(h);
+}
+
+template <typename R>
+gpe_status copy_field(gpe_handle* h, void* dst, const void* src) {
+    typedef typename Cx<R>::T C;
+    k_copy<C><<<blocks_for(h->N, 256), 256, 0, h->st>>>((C*)dst, (const C*)src, h->N);
+    h->launches++;
+    GPE_CUDA(cudaGetLastError());
+    return GPE_OK;
+}
+
+// ---- stepping ----------------------------------------------------------------------------
+template <typename R>
+gpe_status step_real_t(gpe_handle* h, int first, int nsteps, double* obs_out) {
+    GPE_TRY(canonicalize_t<R>(h));
+    h->hb_old_valid = false;
+    const double dt = h->cfg.dt;
+    PassArgs<R> a = base_args<R>(h);
+    a.epi = EPI_RK;
+    a.pro = PRO_PIN;
+    for (int j = 0; j < nsteps; ++j) {
+        const int it = first + j;
+        for (int s = 1; s <= 4; ++s) {
+            a.stage = s;
+            for (int c = 0; c < 2; ++c) a.pin[c] = (s == 1) ? (const typename Cx<R>::T*)h->A[c] : (const typename Cx<R>::T*)h->B[c];
+            // src/oneComponentGPSolver.cu:137-138,155,175,184: m05Idt, mIdt and PARS[T]
+            a.c_re = 0.0;
+            a.c_im = (s <= 2) ? -0.5 * dt : -1.0 * dt;
+            a.t = (s == 1) ? (double)it * dt : (s < 4) ? (it + 0.5) * dt : (double)(it + 1) * dt;
+            a.want_obs = (obs_out != nullptr && j == nsteps - 1 && s == 4) ? 1 : 0;
+            GPE_TRY(run_chain<R>(h, a, h->nf));
+        }
+    }
+    if (obs_out && nsteps > 0) {
+        DevScalars s;
+        GPE_TRY(sync_read_scalars(h, &s));
+        for (int q = 0; q < 3 * h->ncomp; ++q) obs_out[q] = s.obs[q];
+    }
+    return GPE_OK;
+}
+
+template <typename R>
+gpe_status step_imag_t(gpe_handle* h, int first, int nsteps, int* iters_done, int* converged) {
+    typedef typename Cx<R>::T C;
+    const double dt = h->cfg.dt;
+    const bool rk = h->cfg.imag_scheme == GPE_IMAG_RK4;
+    if (rk) {
+        if (h->mode == ST_HB) GPE_TRY(canonicalize_t<R>(h));
+        h->mode = ST_RKI;
+    } else {
+        if (h->mode == ST_RKI) GPE_TRY(canonicalize_t<R>(h));
+        if (!h->hb_old_valid) {
+            GPE_TRY(canonicalize_t<R>(h));
+            for (int c = 0; c < h->ncomp; ++c) GPE_TRY(copy_field<R>(h, h->B[c], h->A[c]));
+            h->hb_old_valid = true;
+        }
+        h->mode = ST_HB;
+    }
+    // Reset the per-call iteration counter.
+    static const int zero = 0;
+    GPE_CUDA(cudaMemcpyAsync(&h->sc->iters_done, &zero, sizeof(int), cudaMemcpyHostToDevice, h->st));
+    PassArgs<R> a = base_args<R>(h);
+    a.check_done = 1;
+    for (int j = 0; j < nsteps; ++j) {
+        const int it = first + j;
+        a.t = (double)it * dt;  // src/oneComponentGPSolver.cu:52 PARS[T] = iteration*dt
+        if (!rk) {
+            a.pro = PRO_CUR;
+            a.epi = EPI_HB;
+            a.stage = 0;
+            GPE_TRY(run_chain<R>(h, a, h->nf));
+        } else {
+            for (int s = 1; s <= 4; ++s) {
+                a.epi = EPI_RKI;
+                a.stage = s;
+                a.pro = (s == 1) ? PRO_A_SCALED : PRO_PIN;
+                for (int c = 0; c < 2; ++c) a.pin[c] = (const C*)h->B[c];
+                a.c_re = (s <= 2) ? -0.5 * dt : -1.0 * dt;
+                a.c_im = 0.0;
+                GPE_TRY(run_chain<R>(h, a, h->nf));
+            }
+        }
+    }
+    DevScalars s;
+    GPE_TRY(sync_read_scalars(h, &s));
+    if (iters_done) *iters_done = s.iters_done;
+    if (converged) *converged = s.converged;
+    if (s.status == GPE_ERR_DIVERGED) return fail(GPE_ERR_DIVERGED, "non-finite norm, energy or chemical potential");
+    return GPE_OK;
+}
+
+template <typename R>
+gpe_status apply_chain_t(gpe_handle* h, int epi, double t, int comp_only) {
+    GPE_TRY(canonicalize_t<R>(h));
+    PassArgs<R> a = base_args<R>(h);
+    a.pro = PRO_PIN;
+    a.epi = epi;
+    a.t = t;
+    int nf = h->nf;
+    if (comp_only >= 0) {  // single component, kinetic only (Laplace / FFT tools)
+        a.ncomp = 1;
+        a.dens = 0;
+        a.pin[0] = (const typename Cx<R>::T*)h->A[comp_only];
+        nf = 1;
+    }
+    for (int q = 0; q < 4; ++q) a.out[q] = (typename Cx<R>::T*)h->O[q];
+    return run_chain<R>(h, a, nf);
+}
+
+template <typename R>
+gpe_status fft_t(gpe_handle* h, int comp, int sign) {
+    typedef typename Cx<R>::T C;
+    GPE_TRY(canonicalize_t<R>(h));
+    PassArgs<R> a = base_args<R>(h);
+    a.ncomp = 1;
+    a.dens = 0;
+    a.pin[0] = (const C*)h->A[comp];
+    a.w[0] = (C*)h->A[comp];
+    a.pro = PRO_PIN;
+    a.epi = EPI_STORE;
+    int axes[2], na = 0;
+    if (h->ny > 1) axes[na++] = 1;
+    if (h->nz > 1) axes[na++] = 2;
+    if (sign < 0) {
+        GPE_TRY(launch_x<R>(h, a, 1, XM_FWD));
+        for (int i = 0; i < na; ++i) GPE_TRY(launch_s<R>(h, a, 1, axes[i], SM_FWD));
+    } else {
+        for (int i = na - 1; i >= 0; --i) GPE_TRY(launch_s<R>(h, a, 1, axes[i], SM_INV));
+        GPE_TRY(launch_x<R>(h, a, 1, XM_INV));
+    }
+    h->hb_old_valid = false;
+    return GPE_OK;
+}
+
+gpe_status check_handle(gpe_handle* h) {
+    if (!h) return fail(GPE_ERR_INVALID_ARG, "null handle");
+    return GPE_OK;
+}
+gpe_status check_comp(gpe_handle* h, int comp) {
+    if (comp < 0 || comp >= h->ncomp) return fail(GPE_ERR_INVALID_ARG, "component index out of range");
+    return GPE_OK;
+}
+
+// Device c128 pointer -> state buffer of comp (conversion for complex64).
+gpe_status upload_c128_device(gpe_handle* h, int comp, const void* dev_c128, void* dst) {
+    if (h->prec == GPE_C128) {
+        GPE_CUDA(cudaMemcpyAsync(dst, dev_c128, 16 * h->N, cudaMemcpyDeviceToDevice, h->st));
+    } else {
+        k_from_c128<float2><<<blocks_for(h->N, 256), 256, 0, h->st>>>((float2*)dst, (const double2*)dev_c128, h->N);
+        h->launches++;
+        GPE_CUDA(cudaGetLastError());
+    }
+    (void)comp;
+    return GPE_OK;
+}
+
+gpe_status upload_c128_host(gpe_handle* h, const double* host, void* dst) {
+    if (h->prec == GPE_C128) {
+        GPE_CUDA(cudaMemcpyAsync(dst, host, 16 * h->N, cudaMemcpyHostToDevice, h->st));
+        GPE_CUDA(cudaStreamSynchronize(h->st));
+        return GPE_OK;
+    }
+    GPE_CUDA(cudaMemcpyAsync(h->stage128, host, 16 * h->N, cudaMemcpyHostToDevice, h->st));
+    GPE_TRY(upload_c128_device(h, 0, h->stage128, dst));
+    GPE_CUDA(cudaStreamSynchronize(h->st));
+    return GPE_OK;
+}
+
+gpe_status download_c128_host(gpe_handle* h, const void* src, double* host) {
+    if (h->prec == GPE_C128) {
+        GPE_CUDA(cudaMemcpyAsync(host, src, 16 * h->N, cudaMemcpyDeviceToHost, h->st));
+    } else {
+        k_to_c128<float2><<<blocks_for(h->N, 256), 256, 0, h->st>>>((double2*)h->stage128, (const float2*)src, h->N);
+        h->launches++;
+        GPE_CUDA(cudaGetLastError());
+        GPE_CUDA(cudaMemcpyAsync(host, h->stage128, 16 * h->N, cudaMemcpyDeviceToHost, h->st));
+    }
+    GPE_CUDA(cudaStreamSynchronize(h->st));
+    return GPE_OK;
+}
+
+gpe_status ensure_out_buffers(gpe_handle* h) {
+    for (int q = 0; q < 2 * h->ncomp; ++q)
+        if (!h->O[q]) GPE_CUDA(cudaMalloc(&h->O[q], h->esz * h->N));
+    return GPE_OK;
+}
+
+void free_all(gpe_handle* h) {
+    void* ptrs[] = {h->A[0], h->A[1], h->B[0], h->B[1], h->K[0], h->K[1], h->V[0], h->V[1], h->W[0], h->W[1],
+                    h->W[2], h->O[0], h->O[1], h->O[2], h->O[3], h->tw[0], h->tw[1], h->tw[2], h->kax[0],
+                    h->kax[1], h->kax[2], h->vdd, h->prms, h->sc, h->partials, h->stage128};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+}
+
+}  // namespace
+
+// ==========================================================================================
+extern "C" {
+
+int gpe_abi_version(void) { return GPE_ABI_VERSION; }
+
+const char* gpe_last_error_string(void) { return g_err.c_str(); }
+
+const char* gpe_status_string(gpe_status s) {
+    switch (s) {
+        case GPE_OK: return "ok";
+        case GPE_ERR_INVALID_ARG: return "invalid argument";
+        case GPE_ERR_UNSUPPORTED: return "unsupported";
+        case GPE_ERR_CUDA: return "CUDA error";
+        case GPE_ERR_OUT_OF_MEMORY: return "out of memory";
+        case GPE_ERR_DIVERGED: return "diverged";
+        case GPE_ERR_TIMEOUT: return "timeout";
+        case GPE_ERR_IO: return "I/O error";
+    }
+    return "unknown status";
+}
+
+gpe_status gpe_config_init(gpe_config* cfg) {
+    if (!cfg) return fail(GPE_ERR_INVALID_ARG, "null config");
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->abi_version = GPE_ABI_VERSION;
+    cfg->nx = cfg->ny = cfg->nz = 1;
+    cfg->dim = 1;
+    cfg->dx[0] = cfg->dx[1] = cfg->dx[2] = 1.0;
+    cfg->ncomp = 1;
+    cfg->precision = GPE_C128;
+    cfg->hamiltonian = GPE_HAM_BEC;
+    cfg->imag_scheme = GPE_IMAG_HEAVYBALL;
+    cfg->npart[0] = cfg->npart[1] = 1.0;
+    return GPE_OK;
+}
+
+int gpe_fft_length_supported(int n) { return (n >= 1 && make_plan(n).ok && length_compiled(n)) ? 1 : 0; }
+
+gpe_status gpe_create(const gpe_config* cfg, gpe_handle** out) {
+    if (!cfg || !out) return fail(GPE_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    if (cfg->abi_version != GPE_ABI_VERSION) return fail(GPE_ERR_INVALID_ARG, "abi_version mismatch");
+    if (cfg->nx < 1 || cfg->ny < 1 || cfg->nz < 1) return fail(GPE_ERR_INVALID_ARG, "grid sizes must be >= 1");
+    if (cfg->ncomp < 1 || cfg->ncomp > 2) return fail(GPE_ERR_INVALID_ARG, "ncomp must be 1 or 2");
+    if (cfg->precision != GPE_C128 && cfg->precision != GPE_C64) return fail(GPE_ERR_INVALID_ARG, "bad precision");
+    if (cfg->hamiltonian < GPE_HAM_BEC || cfg->hamiltonian > GPE_HAM_DIPOLAR)
+        return fail(GPE_ERR_INVALID_ARG, "bad hamiltonian");
+    if (cfg->ncomp == 2 && cfg->hamiltonian != GPE_HAM_BEC2 && cfg->hamiltonian != GPE_HAM_TEMPLATE)
+        return fail(GPE_ERR_UNSUPPORTED, "two components need GPE_HAM_BEC2 or GPE_HAM_TEMPLATE");
+    if (cfg->ncomp == 1 && cfg->hamiltonian == GPE_HAM_BEC2)
+        return fail(GPE_ERR_INVALID_ARG, "GPE_HAM_BEC2 needs two components");
+    if (cfg->imag_scheme != GPE_IMAG_HEAVYBALL && cfg->imag_scheme != GPE_IMAG_RK4)
+        return fail(GPE_ERR_INVALID_ARG, "bad imag_scheme");
+    const int L3[3] = {cfg->nx, cfg->ny, cfg->nz};
+    for (int d = 0; d < 3; ++d)
+        if (!gpe_fft_length_supported(L3[d]))
+            return fail(GPE_ERR_UNSUPPORTED, "grid length " + std::to_string(L3[d]) + " has no compiled FFT plan");
+    if ((long long)cfg->nx * cfg->ny * cfg->nz > (1LL << 31))
+        return fail(GPE_ERR_UNSUPPORTED, "grid larger than 2^31 points");
+
+    gpe_handle* h = new gpe_handle();
+    h->cfg = *cfg;
+    h->prec = cfg->precision;
+    h->nx = cfg->nx;
+    h->ny = cfg->ny;
+    h->nz = cfg->nz;
+    h->N = (long long)cfg->nx * cfg->ny * cfg->nz;
+    h->ncomp = cfg->ncomp;
+    h->dens = cfg->hamiltonian == GPE_HAM_DIPOLAR ? 1 : 0;
+    h->nf = h->ncomp + h->dens;
+    h->esz = h->prec == GPE_C128 ? 16 : 8;
+
+    auto bail = [&](gpe_status s) {
+        free_all(h);
+        delete h;
+        return s;
+    };
+    auto dmalloc = [&](void** p, size_t bytes) -> bool {
+        cudaError_t e = cudaMalloc(p, bytes);
+        if (e != cudaSuccess) {
+            g_err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+            return false;
+        }
+        return true;
+    };
+    const size_t fb = h->esz * h->N;
+    for (int c = 0; c < h->ncomp; ++c) {
+        if (!dmalloc(&h->A[c], fb) || !dmalloc(&h->B[c], fb) || !dmalloc(&h->K[c], fb) || !dmalloc(&h->V[c], fb))
+            return bail(GPE_ERR_OUT_OF_MEMORY);
+        cudaMemsetAsync(h->A[c], 0, fb, h->st);
+        cudaMemsetAsync(h->B[c], 0, fb, h->st);
+        cudaMemsetAsync(h->K[c], 0, fb, h->st);
+        cudaMemsetAsync(h->V[c], 0, fb, h->st);
+    }
+    for (int f = 0; f < h->nf; ++f)
+        if (!dmalloc(&h->W[f], fb)) return bail(GPE_ERR_OUT_OF_MEMORY);
+    if (h->prec == GPE_C64 && !dmalloc(&h->stage128, 16 * h->N)) return bail(GPE_ERR_OUT_OF_MEMORY);
+
+    // Twiddles, k axes, dipolar kernel, parameters, scalars, partial sums.
+    std::vector<double> kax[3];
+    host_kaxes(*cfg, kax);
+    for (int d = 0; d < 3; ++d) {
+        if (!dmalloc((void**)&h->kax[d], sizeof(double) * L3[d])) return bail(GPE_ERR_OUT_OF_MEMORY);
+        cudaMemcpy(h->kax[d], kax[d].data(), sizeof(double) * L3[d], cudaMemcpyHostToDevice);
+        if (h->prec == GPE_C128) {
+            std::vector<double2> tw;
+            host_twiddles(L3[d], tw);
+            if (!dmalloc(&h->tw[d], sizeof(double2) * L3[d])) return bail(GPE_ERR_OUT_OF_MEMORY);
+            cudaMemcpy(h->tw[d], tw.data(), sizeof(double2) * L3[d], cudaMemcpyHostToDevice);
+        } else {
+            std::vector<float2> tw;
+            host_twiddles(L3[d], tw);
+            if (!dmalloc(&h->tw[d], sizeof(float2) * L3[d])) return bail(GPE_ERR_OUT_OF_MEMORY);
+            cudaMemcpy(h->tw[d], tw.data(), sizeof(float2) * L3[d], cudaMemcpyHostToDevice);
+        }
+    }
+    if (h->dens) {
+        std::vector<double> v;
+        host_vdd(*cfg, kax, v);
+        if (h->prec == GPE_C128) {
+            if (!dmalloc(&h->vdd, sizeof(double) * h->N)) return bail(GPE_ERR_OUT_OF_MEMORY);
+            cudaMemcpy(h->vdd, v.data(), sizeof(double) * h->N, cudaMemcpyHostToDevice);
+        } else {
+            std::vector<float> vf(v.begin(), v.end());
+            if (!dmalloc(&h->vdd, sizeof(float) * h->N)) return bail(GPE_ERR_OUT_OF_MEMORY);
+            cudaMemcpy(h->vdd, vf.data(), sizeof(float) * h->N, cudaMemcpyHostToDevice);
+        }
+    }
+    if (!dmalloc((void**)&h->prms, sizeof(double) * GPE_NO_HAMIL_PARAMS)) return bail(GPE_ERR_OUT_OF_MEMORY);
+    cudaMemcpy(h->prms, cfg->prms, sizeof(double) * GPE_NO_HAMIL_PARAMS, cudaMemcpyHostToDevice);
+    if (!dmalloc((void**)&h->sc, sizeof(DevScalars))) return bail(GPE_ERR_OUT_OF_MEMORY);
+    {
+        DevScalars s;
+        std::memset(&s, 0, sizeof(s));
+        s.scale[0][0] = s.scale[0][1] = s.scale[1][0] = s.scale[1][1] = 1.0;
+        s.norm[0] = cfg->npart[0];
+        s.norm[1] = cfg->npart[1];
+        cudaMemcpy(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice);
+    }
+    const int B = 256 / plan_T(h->nx) > 0 ? 256 / plan_T(h->nx) : 1;
+    const size_t nblk = (size_t)(h->ny * h->nz + B - 1) / B;
+    if (!dmalloc((void**)&h->partials, nblk * MAXQ * 2 * sizeof(double))) return bail(GPE_ERR_OUT_OF_MEMORY);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        g_err = std::string("gpe_create: ") + cudaGetErrorString(e);
+        return bail(GPE_ERR_CUDA);
+    }
+    *out = h;
+    return GPE_OK;
+}
+
+gpe_status gpe_destroy(gpe_handle* h) {
+    if (!h) return GPE_OK;
+    cudaStreamSynchronize(h->st);
+    free_all(h);
+    delete h;
+    return GPE_OK;
+}
+
+gpe_status gpe_set_stream(gpe_handle* h, void* stream) {
+    GPE_TRY(check_handle(h));
+    h->st = (cudaStream_t)stream;
+    return GPE_OK;
+}
+
+gpe_status gpe_set_params(gpe_handle* h, const double prms[GPE_NO_HAMIL_PARAMS]) {
+    GPE_TRY(check_handle(h));
+    if (!prms) return fail(GPE_ERR_INVALID_ARG, "null prms");
+    std::memcpy(h->cfg.prms, prms, sizeof(double) * GPE_NO_HAMIL_PARAMS);
+    GPE_CUDA(cudaMemcpyAsync(h->prms, h->cfg.prms, sizeof(double) * GPE_NO_HAMIL_PARAMS, cudaMemcpyHostToDevice, h->st));
+    if (h->dens) {
+        std::vector<double> kax[3], v;
+        host_kaxes(h->cfg, kax);
+        host_vdd(h->cfg, kax, v);
+        GPE_CUDA(cudaStreamSynchronize(h->st));
+        if (h->prec == GPE_C128) {
+            GPE_CUDA(cudaMemcpy(h->vdd, v.data(), sizeof(double) * h->N, cudaMemcpyHostToDevice));
+        } else {
+            std::vector<float> vf(v.begin(), v.end());
+            GPE_CUDA(cudaMemcpy(h->vdd, vf.data(), sizeof(float) * h->N, cudaMemcpyHostToDevice));
+        }
+    }
+    GPE_CUDA(cudaStreamSynchronize(h->st));
+    return GPE_OK;
+}
+
+gpe_status gpe_set_psi(gpe_handle* h, int comp, const double* host_c128) {
+    GPE_TRY(check_handle(h));
+    GPE_TRY(check_comp(h, comp));
+    if (!host_c128) return fail(GPE_ERR_INVALID_ARG, "null psi");
+    GPE_TRY(canonicalize(h));
+    GPE_TRY(upload_c128_host(h, host_c128, h->A[comp]));
+    GPE_CUDA(cudaMemcpyAsync(h->B[comp], h->A[comp], h->esz * h->N, cudaMemcpyDeviceToDevice, h->st));
+    GPE_CUDA(cudaStreamSynchronize(h->st));
+    h->hb_old_valid = true;
+    return GPE_OK;
+}
+
+gpe_status gpe_set_psi_device(gpe_handle* h, int comp, const void* dev_c128) {
+    GPE_TRY(check_handle(h));
+    GPE_TRY(check_comp(h, comp));
+    if (!dev_c128) return fail(GPE_ERR_INVALID_ARG, "null psi");
+    GPE_TRY(canonicalize(h));
+    GPE_TRY(upload_c128_device(h, comp, dev_c128, h->A[comp]));
+    GPE_CUDA(cudaMemcpyAsync(h->B[comp], h->A[comp], h->esz * h->N, cudaMemcpyDeviceToDevice, h->st));
+    h->hb_old_valid = true;
+    return GPE_OK;
+}
+
+gpe_status gpe_get_psi(gpe_handle* h, int comp, double* host_c128) {
+    GPE_TRY(check_handle(h));
+    GPE_TRY(check_comp(h, comp));
+    if (!host_c128) return fail(GPE_ERR_INVALID_ARG, "null output");
+    GPE_TRY(canonicalize(h));
+    return download_c128_host(h, h->A[comp], host_c128);
+}
+
+gpe_status gpe_get_psi_device(gpe_handle* h, int comp, void* dev_c128) {
+    GPE_TRY(check_handle(h));
+    GPE_TRY(check_comp(h, comp));
+    if (!dev_c128) return fail(GPE_ERR_INVALID_ARG, "null output");
+    GPE_TRY(canonicalize(h));
+    if (h->prec == GPE_C128) {
+        GPE_CUDA(cudaMemcpyAsync(dev_c128, h->A[comp], 16 * h->N, cudaMemcpyDeviceToDevice, h->st));
+    } else {
+        k_to_c128<float2><<<blocks_for(h->N, 256), 256, 0, h->st>>>((double2*)dev_c128, (const float2*)h->A[comp], h->N);
+        h->launches++;
+        GPE_CUDA(cudaGetLastError());
+    }
+    return GPE_OK;
+}
+
+gpe_status gpe_set_vext(gpe_handle* h, int comp, const double* host_c128) {
+    GPE_TRY(check_handle(h));
+    GPE_TRY(check_comp(h, comp));
+    if (!host_c128) return fail(GPE_ERR_INVALID_ARG, "null vext");
+    return upload_c128_host(h, host_c128, h->V[comp]);
+}
+
+gpe_status gpe_step_real(gpe_handle* h, int first_iteration, int nsteps, double* obs_out) {
+    GPE_TRY(check_handle(h));
+    if (nsteps < 0) return fail(GPE_ERR_INVALID_ARG, "nsteps < 0");
+    return h->prec == GPE_C64 ? step_real_t<float>(h, first_iteration, nsteps, obs_out)
+                              : step_real_t<double>(h, first_iteration, nsteps, obs_out);
+}
+
+gpe_status gpe_step_imag(gpe_handle* h, int first_iteration, int nsteps, int* iters_done, int* converged) {
+    GPE_TRY(check_handle(h));
+    if (nsteps < 0) return fail(GPE_ERR_INVALID_ARG, "nsteps < 0");
+    return h->prec == GPE_C64 ? step_imag_t<float>(h, first_iteration, nsteps, iters_done, converged)
+                              : step_imag_t<double>(h, first_iteration, nsteps, iters_done, converged);
+}
+
+gpe_status gpe_imag_state(gpe_handle* h, double* out) {
+    GPE_TRY(check_handle(h));
+    if (!out) return fail(GPE_ERR_INVALID_ARG, "null output");
+    DevScalars s;
+    GPE_TRY(sync_read_scalars(h, &s));
+    for (int c = 0; c < h->ncomp; ++c) {
+        out[4 * c + 0] = s.norm[c];
+        out[4 * c + 1] = s.mu[c];
+        out[4 * c + 2] = s.en[c];
+        out[4 * c + 3] = s.en_prev[c];
+    }
+    return GPE_OK;
+}
+
+gpe_status gpe_reset_imag_state(gpe_handle* h) {
+    GPE_TRY(check_handle(h));
+    DevScalars s;
+    GPE_TRY(sync_read_scalars(h, &s));
+    for (int c = 0; c < 2; ++c) {
+        s.mu[c] = s.en[c] = s.en_prev[c] = s.mu_prev[c] = 0.0;
+        s.norm[c] = h->cfg.npart[c];
+    }
+    s.done = s.converged = s.iters_done = s.status = s.have_mu_prev = 0;
+    s.counter = 0;
+    GPE_CUDA(cudaMemcpyAsync(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice, h->st));
+    GPE_CUDA(cudaStreamSynchronize(h->st));
+    return GPE_OK;
+}
+
+gpe_status gpe_laplace(gpe_handle* h, int comp, double* host_out_c128) {
+    GPE_TRY(check_handle(h));
+    GPE_TRY(check_comp(h, comp));
+    if (!host_out_c128) return fail(GPE_ERR_INVALID_ARG, "null output");
+    GPE_TRY(h->prec == GPE_C64 ? apply_chain_t<float>(h, EPI_STORE, 0.0, comp)
+                               : apply_chain_t<double>(h, EPI_STORE, 0.0, comp));
+    return download_c128_host(h, h->W[0], host_out_c128);
+}
+
+gpe_status gpe_apply_h(gpe_handle* h, double t, int comp, double* hmu, double* hen) {
+    GPE_TRY(check_handle(h));
+    GPE_TRY(check_comp(h, comp));
+    GPE_TRY(ensure_out_buffers(h));
+    GPE_TRY(h->prec == GPE_C64 ? apply_chain_t<float>(h, EPI_APPLYH, t, -1)
+                               : apply_chain_t<double>(h, EPI_APPLYH, t, -1));
+    if (hmu) GPE_TRY(download_c128_host(h, h->O[2 * comp], hmu));
+    if (hen) GPE_TRY(download_c128_host(h, h->O[2 * comp + 1], hen));
+    return GPE_OK;
+}
+
+gpe_status gpe_observables(gpe_handle* h, double t, double* out) {
+    GPE_TRY(check_handle(h));
+    if (!out) return fail(GPE_ERR_INVALID_ARG, "null output");
+    GPE_TRY(h->prec == GPE_C64 ? apply_chain_t<float>(h, EPI_OBS, t, -1) : apply_chain_t<double>(h, EPI_OBS, t, -1));
+    DevScalars s;
+    GPE_TRY(sync_read_scalars(h, &s));
+    for (int q = 0; q < 3 * h->ncomp; ++q) out[q] = s.obs[q];
+    if (s.status == GPE_ERR_DIVERGED) return fail(GPE_ERR_DIVERGED, "non-finite observable");
+    return GPE_OK;
+}
+
+gpe_status gpe_fft(gpe_handle* h, int comp, int sign) {
+    GPE_TRY(check_handle(h));
+    GPE_TRY(check_comp(h, comp));
+    if (sign != -1 && sign != 1) return fail(GPE_ERR_INVALID_ARG, "sign must be -1 or +1");
+    return h->prec == GPE_C64 ? fft_t<float>(h, comp, sign) : fft_t<double>(h, comp, sign);
+}
+
+gpe_status gpe_sync(gpe_handle* h) {
+    GPE_TRY(check_handle(h));
+    GPE_CUDA(cudaStreamSynchronize(h->st));
+    GPE_CUDA(cudaGetLastError());
+    return GPE_OK;
+}
+
+long long gpe_kernel_launches(const gpe_handle* h) { return h ? h->launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,7 @@
+// Pass-kernel instantiations: length family p2, float.
+#include "gpe_sizes.h"
+#define GPE_R float
+#define GPE_SFX f
+#define GPE_FAM p2
+#define GPE_SIZES(X) GPE_SIZES_p2(X)
+#include "gpe_inst_body.cuh"

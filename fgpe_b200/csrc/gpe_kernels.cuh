@@ -1,0 +1,276 @@
+// gpe_kernels.cuh -- fused axis-pass kernels of the GPE step.
+//
+// One stage of the reference's RK4 step is cuFFT-forward -> Laplace ->
+// cuFFT-inverse -> plugin pointwise kernel -> 1..2 stage kernels
+// (src/oneComponentGPSolver.cu:170-187, src/baseHamiltonian.cu:86-96).  Here a
+// stage is a chain of axis passes over the 3D field (x fastest):
+//
+//   X_FWD  rows along x: prologue (stage state, lazy renormalisation,
+//          dipolar density) + forward x-FFT                      -> W
+//   S_FWD  strided lines (y) forward                               W -> W
+//   S_FKI  last strided axis: forward FFT, k-space multiply (kinetic
+//          2 pi^2 k^2/N, dipolar V(k)/N), inverse FFT              W -> W
+//   S_INV  strided lines inverse                                   W -> W
+//   X_INV  rows along x: inverse x-FFT + epilogue (Hamiltonian plugin
+//          term, RK4 / heavy-ball stage arithmetic, FP64 compensated
+//          reductions with a last-block device finalize)
+//
+// and X_FULL does all of it in one kernel when x is the only axis.
+#pragma once
+
+#include "gpe_common.cuh"
+#include "gpe_fft.cuh"
+#include "../../include/gpe.h"
+
+namespace gpe {
+
+enum PassMode { XM_FWD = 0, XM_INV = 1, XM_FULL = 2, SM_FWD = 3, SM_INV = 4, SM_FKI = 5 };
+// Prologue / epilogue psi source.
+enum ProOp {
+    PRO_PIN = 0,      // psi = pin[c]
+    PRO_CUR = 1,      // psi = scale[cur][c] * buf[cur][c]        (heavy ball)
+    PRO_A_SCALED = 2  // psi = scale[cur][c] * buf[0][c]          (RK4 imaginary, stage 1)
+};
+enum EpiOp {
+    EPI_STORE = 0,   // W <- inverse transform (gpe_fft, gpe_laplace)
+    EPI_RK = 1,      // real-time RK4 stage
+    EPI_HB = 2,      // heavy-ball imaginary step + renormalisation reductions
+    EPI_APPLYH = 3,  // out <- h_mu, h_en
+    EPI_OBS = 4,     // reductions of |psi|^2, Re(psi* h_mu), Re(psi* h_en)
+    EPI_RKI = 5      // imaginary-time RK4 stage
+};
+enum SpecOp { SPEC_NONE = 0, SPEC_KIN = 1 };
+
+constexpr int MAXQ = 6;  // reduced quantities per launch (3 per component)
+
+template <typename R>
+struct PassArgs {
+    typedef typename Cx<R>::T C;
+    int nx, ny, nz;
+    int nrows;               // X pass: rows = ny*nz
+    int ncomp;               // 1 or 2
+    int dens;                // 1: field index ncomp is the dipolar density
+    int tx;                  // strided pass: lines (x values) per CTA
+    int mode, pro, epi, spec, stage, ham, sax;
+    int check_done;          // exit when sc->done is set (stepping chunks)
+    int want_obs;            // RK stage 4: logging reductions
+    C* w[3];                 // transformed fields (work buffers)
+    C* buf[2][2];            // [slot][comp] state buffers (A = slot 0, B = slot 1)
+    C* kacc[2];              // RK accumulators
+    const C* pin[2];         // PRO_PIN source
+    const C* vext[2];
+    C* out[4];               // EPI_APPLYH: h_mu c0, h_en c0, h_mu c1, h_en c1
+    const C* tw;             // roots of unity for this pass's length
+    const double* kx;
+    const double* ky;
+    const double* kz;
+    const R* vdd;            // dipolar kernel / N (spectral order) or null
+    const double* prms;      // d_h_params
+    DevScalars* sc;
+    double* partials;        // [gridDim.x][MAXQ][2]
+    long long sstride;       // strided pass: element stride along the line
+    long long ostride;       // strided pass: stride of blockIdx.y
+    double t;                // Hamiltonian time (BEC quench)
+    double dt, beta, lap_scale, DV, eps;
+    double npart[2];
+    double c_re, c_im;       // RK stage coefficient (stage 1..3 axpy; final uses c/6)
+};
+
+// ---- shared-memory line addressing -----------------------------------------
+template <typename C> struct RowAddr {      // X pass: S[b*L + pos]
+    C* base;
+    __device__ __forceinline__ C* operator()(int pos) const { return base + pos; }
+};
+template <typename C> struct ColAddr {      // strided pass: S[pos*tx + b]
+    C* base;
+    int tx;
+    __device__ __forceinline__ C* operator()(int pos) const { return base + pos * tx; }
+};
+
+// ---- compensated FP64 reductions --------------------------------------------
+struct DD {
+    double s, c;
+};
+__device__ __forceinline__ DD dd_add(DD a, double v) {
+    double t = a.s + v;
+    double e = (fabs(a.s) >= fabs(v)) ? (a.s - t) + v : (v - t) + a.s;
+    return DD{t, a.c + e};
+}
+__device__ __forceinline__ DD dd_merge(DD a, DD b) {
+    DD r = dd_add(a, b.s);
+    r.c += b.c;
+    return r;
+}
+
+// Block-wide deterministic reduction of NQ compensated sums; result valid in
+// thread 0.  red: shared scratch of 32*NQ DD.
+// The last warp may be partial (line lengths with T = 3, 9, ... threads per
+// line): shuffles use the mask of the lanes that exist.
+template <int NQ>
+__device__ __forceinline__ void block_reduce(DD (&acc)[NQ], DD* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = (blockDim.x + 31) >> 5;
+    const int wl = min(32, (int)blockDim.x - warp * 32);
+    const unsigned mask = (wl == 32) ? 0xffffffffu : ((1u << wl) - 1u);
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            DD o;
+            o.s = __shfl_down_sync(mask, acc[q].s, off);
+            o.c = __shfl_down_sync(mask, acc[q].c, off);
+            if (lane + off < wl) acc[q] = dd_merge(acc[q], o);
+        }
+    }
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) red[warp * NQ + q] = acc[q];
+    __syncthreads();
+    if (warp == 0) {
+        const int wl0 = min(32, (int)blockDim.x);
+        const unsigned mask0 = (wl0 == 32) ? 0xffffffffu : ((1u << wl0) - 1u);
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            DD v = (lane < nwarps) ? red[lane * NQ + q] : DD{0.0, 0.0};
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                DD o;
+                o.s = __shfl_down_sync(mask0, v.s, off);
+                o.c = __shfl_down_sync(mask0, v.c, off);
+                if (lane + off < wl0) v = dd_merge(v, o);
+            }
+            acc[q] = v;
+        }
+    }
+    __syncthreads();
+}
+
+// d_quench_as, hamiltonians/BEC_oneComponent.cu:167-178.
+__device__ __forceinline__ double quench_as(double time, const double* prms) {
+    double a0 = prms[0], a1 = prms[1], a2 = prms[2];
+    double t1 = prms[3], t2 = prms[4], t3 = prms[5];
+    if (0 < time && time <= t1) return a0 + (a1 - a0) / (t1)*time;
+    if (t1 < time && time <= t2) return a1;
+    if (t2 < time && time <= t3) return a1 + (a2 - a1) / (t3 - t2) * (time - t2);
+    return a2;
+}
+
+// hpp/header.hpp:27 pi literal.
+#define GPE_PI_REF 3.141592653589793
+
+// Pointwise Hamiltonian term.  T = kinetic part (the reference's d_hpsi after
+// alg_Laplace), psi, V, phi (dipolar mean field).  Writes h_mu and, when
+// want_en, h_en.  Formulas and evaluation order follow
+//  BEC     hamiltonians/BEC_oneComponent.cu:128-165
+//  BEC2    hamiltonians/BEC_twoComponent.cu:168-244 (en variant keeps the
+//          vext1[ix].y read of line 208 for component 2)
+//  TEMPLATE hamiltonians/single_template.cu:333-373.
+template <typename R>
+struct HamCoef {
+    R g_en, g_mu;                  // BEC: 2 pi a, 4 pi a
+    R g11e, g12e, g22e, g11m, g12m, g22m;
+};
+
+template <typename R, typename C>
+__device__ __forceinline__ void ham_point(int ham, int ncomp, const HamCoef<R>& hc, const C* psi, const C* T,
+                                          const C* V, R phi, bool want_en, C* hmu, C* hen) {
+    if (ham == GPE_HAM_BEC || ham == GPE_HAM_DIPOLAR) {
+        const R px = psi[0].x, py = psi[0].y;
+        const R n = px * px + py * py;
+        R rX, rY;
+        if (want_en) {
+            rX = (V[0].x + hc.g_en * n) + (R)0.5 * phi;
+            rY = V[0].y;
+            hen[0] = mk(T[0].x + rX * px - rY * py, T[0].y + rX * py + rY * px);
+        }
+        rX = (V[0].x + hc.g_mu * n) + phi;
+        rY = V[0].y;
+        hmu[0] = mk(T[0].x + rX * px - rY * py, T[0].y + rX * py + rY * px);
+    } else if (ham == GPE_HAM_BEC2) {
+        const R x1 = psi[0].x, y1 = psi[0].y, x2 = psi[1].x, y2 = psi[1].y;
+        const R n1 = x1 * x1 + y1 * y1, n2 = x2 * x2 + y2 * y2;
+        R aX, aY;
+        if (want_en) {
+            aX = (V[0].x + hc.g11e * n1 + hc.g12e * n2);
+            aY = V[0].y;
+            hen[0] = mk(T[0].x + aX * x1 - aY * y1, T[0].y + aX * y1 + aY * x1);
+        }
+        aX = (V[0].x + hc.g11m * n1 + hc.g12m * n2);
+        aY = V[0].y;
+        hmu[0] = mk(T[0].x + (aX * x1 - aY * y1), T[0].y + (aX * y1 + aY * x1));
+        if (want_en) {
+            aX = (V[1].x + hc.g22e * n2 + hc.g12e * n1);
+            aY = V[1].y;
+            hen[1] = mk(T[1].x + aX * x2 - aY * y2, T[1].y + aX * y2 + aY * x2);
+            aX = (V[1].x + hc.g22m * n2 + hc.g12m * n1);
+            aY = V[0].y;  // hamiltonians/BEC_twoComponent.cu:208
+        } else {
+            aX = (V[1].x + hc.g22m * n2 + hc.g12m * n1);
+            aY = V[1].y;
+        }
+        hmu[1] = mk(T[1].x + (aX * x2 - aY * y2), T[1].y + (aX * y2 + aY * x2));
+    } else {
+        for (int c = 0; c < ncomp; ++c) {
+            hmu[c] = T[c];
+            if (want_en) hen[c] = T[c];
+        }
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ HamCoef<R> make_coef(const PassArgs<R>& a) {
+    HamCoef<R> hc;
+    double q = (a.ham == GPE_HAM_BEC || a.ham == GPE_HAM_DIPOLAR) ? quench_as(a.t, a.prms) : 0.0;
+    hc.g_en = (R)(2 * GPE_PI_REF * q);
+    hc.g_mu = (R)(4 * GPE_PI_REF * q);
+    const double a11 = a.prms[0], a22 = a.prms[1], a12 = a.prms[2];
+    hc.g11e = (R)(2 * GPE_PI_REF * a11);
+    hc.g12e = (R)(2 * GPE_PI_REF * a12);
+    hc.g22e = (R)(2 * GPE_PI_REF * a22);
+    hc.g11m = (R)(4 * GPE_PI_REF * a11);
+    hc.g12m = (R)(4 * GPE_PI_REF * a12);
+    hc.g22m = (R)(4 * GPE_PI_REF * a22);
+    return hc;
+}
+
+// Exact-form helpers in FP64 for the stage arithmetic.
+__device__ __forceinline__ double2 to_d(float2 v) { return make_double2(v.x, v.y); }
+__device__ __forceinline__ double2 to_d(double2 v) { return v; }
+template <typename C> __device__ __forceinline__ C from_d(double2 v);
+template <> __device__ __forceinline__ float2 from_d<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
+template <> __device__ __forceinline__ double2 from_d<double2>(double2 v) { return v; }
+
+// UpdateRKStep, complex overload (src/parallel.cu:238-244).
+__device__ __forceinline__ double2 rk_axpy(double2 old, double cr, double ci, double2 h) {
+    return make_double2(old.x + (cr * h.x - ci * h.y), old.y + (cr * h.y + ci * h.x));
+}
+// FinalRKStep (src/parallel.cu:261-271).
+__device__ __forceinline__ double2 rk_final(double2 old, double cr, double ci, double2 k, double2 h) {
+    double aX = k.x + h.x, aY = k.y + h.y;
+    return make_double2(old.x + (cr * aX - ci * aY) / 6.0, old.y + (cr * aY + ci * aX) / 6.0);
+}
+
+// ---- last-block finalize ------------------------------------------------------
+// Called by every block after its own reduction (thread 0 holds acc).
+template <typename R, int NQ>
+__device__ void reduce_and_finalize(const PassArgs<R>& a, DD (&acc)[NQ], DD* red);
+
+template <typename R>
+__device__ void finalize_scalars(const PassArgs<R>& a, const double* S);
+
+// ---- kernels ----------------------------------------------------------------
+template <typename R, int L>
+struct XCfg {
+    static constexpr int T = Plan<L>::T;
+    static constexpr int B = (256 / T) > 0 ? (256 / T) : 1;  // rows per CTA
+    static constexpr int THREADS = B * T;
+};
+
+template <typename R, int L, int NF>
+__global__ void __launch_bounds__(256) k_xpass(PassArgs<R> a);
+
+template <typename R, int L, int NF>
+__global__ void __launch_bounds__(512) k_spass(PassArgs<R> a);
+
+}  // namespace gpe

@@ -1,0 +1,192 @@
+/*
+ * gpe.h -- C ABI of the B200-native Gross-Pitaevskii solver (libgpe.so).
+ *
+ * The reference (fGPE v0.3) exposes its hot path as a C++ class hierarchy,
+ * not an FFI:  Cuda <- BaseHamiltonian <- OneComponentGPSolver /
+ * TwoComponentGPSolver <- BEConeComponent / BECtwoComponent / SingleTemplate.
+ * Every entry point below replaces one member (or one member sequence) of that
+ * hierarchy; the replaced reference interface is cited beside each one as
+ * path:line inside the reference project.  The C++ plugin classes in
+ * fgpe_b200/host/ call these functions the way the reference's plugins call
+ * their base-class members.
+ *
+ * Conventions
+ *  - Every call returns gpe_status; GPE_OK is 0.  On failure
+ *    gpe_last_error_string() returns a one-line message (thread-local).
+ *    Nothing here calls exit(); the reference exits on a missing key
+ *    (src/input_variables.cu:171-209) and prints-and-continues on CUDA errors
+ *    (src/parallel.cu:7-11, CCE).
+ *  - Host wavefunction / potential buffers are interleaved complex128
+ *    (re, im pairs of double), index z*NX*NY + y*NX + x (hpp/header.hpp:20,
+ *    ID macro), i.e. exactly the bytes of a .wdat file
+ *    (src/output.cu:262-277).  The complex64 form converts on the device.
+ *  - A handle owns its device buffers; it is not thread-shared, distinct
+ *    handles are independent.  All GPU work of a handle is issued on the
+ *    stream set by gpe_set_stream (default: the legacy default stream).
+ *  - Units are the reference's code units: lengths in a_ho, time in 1/omega_ho,
+ *    energies in hbar*omega_ho (src/params.cu:223-279).
+ */
+#ifndef GPE_B200_GPE_H
+#define GPE_B200_GPE_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPE_ABI_VERSION 1
+/* hpp/header.hpp:23  NO_HAMIL_PARAMS: size of d_h_params */
+#define GPE_NO_HAMIL_PARAMS 32
+
+typedef enum gpe_status {
+    GPE_OK = 0,
+    GPE_ERR_INVALID_ARG = 1,   /* null pointer, bad component, bad enum   */
+    GPE_ERR_UNSUPPORTED = 2,   /* grid length with no FFT plan, option off */
+    GPE_ERR_CUDA = 3,          /* a CUDA runtime call failed               */
+    GPE_ERR_OUT_OF_MEMORY = 4, /* device or pinned allocation failed       */
+    GPE_ERR_DIVERGED = 5,      /* NaN/Inf seen by the device watchdog      */
+    GPE_ERR_TIMEOUT = 6,       /* a bounded device wait gave up            */
+    GPE_ERR_IO = 7             /* file could not be opened / short read    */
+} gpe_status;
+
+/* Storage / arithmetic form of the fields.
+ *  GPE_C128: complex128 everywhere (the drop-in; cuFFT Z2Z in the reference,
+ *            src/parallel.cu:97-102).
+ *  GPE_C64 : complex64 fields and FFT butterflies; stage axpy coefficients,
+ *            norm, energy, chemical potential, renormalisation and the
+ *            convergence test stay FP64 (compensated sums). */
+typedef enum gpe_precision { GPE_C128 = 0, GPE_C64 = 1 } gpe_precision;
+
+/* Which Hamiltonian plugin supplies the pointwise term.
+ *  GPE_HAM_BEC      hamiltonians/BEC_oneComponent.cu:128-178 (prms[0..5] = quench a0,a1,a2,t1,t2,t3)
+ *  GPE_HAM_BEC2     hamiltonians/BEC_twoComponent.cu:168-244 (prms[0..2] = a11,a22,a12)
+ *  GPE_HAM_TEMPLATE hamiltonians/single_template.cu:333-373  (h = T only)
+ *  GPE_HAM_DIPOLAR  GPE_HAM_BEC plus a k-space dipolar term; prms[6] = a_dd,
+ *                   prms[7..9] = dipole direction, prms[10] = spherical
+ *                   real-space cut-off radius R (0 = no cut-off).  The kernel
+ *                   is 12*pi*a_dd*((k.d)^2/k^2 - 1/3) as in
+ *                   src/parallel.cu:326-352 (never called there), times
+ *                   1 + 3cos(kR)/(kR)^2 - 3sin(kR)/(kR)^3 with k in rad/length. */
+typedef enum gpe_hamiltonian {
+    GPE_HAM_BEC = 0,
+    GPE_HAM_BEC2 = 1,
+    GPE_HAM_TEMPLATE = 2,
+    GPE_HAM_DIPOLAR = 3
+} gpe_hamiltonian;
+
+/* Imaginary-time scheme.
+ *  GPE_IMAG_HEAVYBALL  the reference's scheme, src/parallel.cu:294-302 with the
+ *                      loop of src/oneComponentGPSolver.cu:46-95 (1 component)
+ *                      and src/twoComponentGPSolver.cu:35-105 (2 components).
+ *  GPE_IMAG_RK4        classic RK4 on d(psi)/d(tau) = -H psi, renormalised to
+ *                      npart after every step; mu and E of the normalised
+ *                      state; converged when |mu_n - mu_{n-1}| < epsilon_e.
+ *                      Not in the reference (its imaginary time is not RK4). */
+typedef enum gpe_imag_scheme { GPE_IMAG_HEAVYBALL = 0, GPE_IMAG_RK4 = 1 } gpe_imag_scheme;
+
+typedef struct gpe_config {
+    int    abi_version;          /* must be GPE_ABI_VERSION                     */
+    int    nx, ny, nz;           /* Params::NX[3]   hpp/params.hpp:23          */
+    int    dim;                  /* Params::DIM     src/params.cu:145-154      */
+    double xmax[3];              /* Params::XMAX, code units                   */
+    double dx[3];                /* Params::DX, code units                     */
+    int    ncomp;                /* 1 or 2                                      */
+    int    precision;            /* gpe_precision                              */
+    int    hamiltonian;          /* gpe_hamiltonian                            */
+    int    imag_scheme;          /* gpe_imag_scheme                            */
+    double prms[GPE_NO_HAMIL_PARAMS]; /* d_h_params, hpp/parallel.hpp:39      */
+    double dt;                   /* code units: p.dt*p.omho/1000               */
+    double beta;                 /* heavy-ball momentum, input key "beta"      */
+    double npart[2];             /* norm targets, Params::npart / npart1,2     */
+    double epsilon_e;            /* convergence threshold, input "epsilon_e"   */
+    int    reserved[8];          /* must be zero                                */
+} gpe_config;
+
+typedef struct gpe_handle gpe_handle;
+
+/* ---- library ---------------------------------------------------------- */
+int         gpe_abi_version(void);
+const char* gpe_last_error_string(void);
+const char* gpe_status_string(gpe_status s);
+/* Fill cfg with defaults (abi_version set, 1 component, C128, BEC, heavy-ball). */
+gpe_status  gpe_config_init(gpe_config* cfg);
+/* 1 when a grid length has a device FFT plan (products of 2, 3 and 5 up to
+ * 1024 whose plan needs at most 24 values per thread), else 0. */
+int         gpe_fft_length_supported(int n);
+
+/* ---- lifecycle: replaces Cuda::Cuda / ~Cuda (src/parallel.cu:14-113,
+ * hpp/parallel.hpp:80-126) and BaseHamiltonian::InitializeKspace/Space
+ * (src/baseHamiltonian.cu:25-82). ---------------------------------------- */
+gpe_status gpe_create(const gpe_config* cfg, gpe_handle** out);
+gpe_status gpe_destroy(gpe_handle* h);
+/* cudaStream_t passed as void*; NULL = legacy default stream. */
+gpe_status gpe_set_stream(gpe_handle* h, void* cuda_stream);
+/* Replaces the H2D copy of d_h_params (hamiltonians/BEC_oneComponent.cu:15). */
+gpe_status gpe_set_params(gpe_handle* h, const double prms[GPE_NO_HAMIL_PARAMS]);
+
+/* ---- data in / out: replaces the cudaMemcpyAsync calls of
+ * src/oneComponentGPSolver.cu:32-34,127-129,98,211 and
+ * src/twoComponentGPSolver.cu:23-28,107-108. comp is 0 or 1. ------------- */
+/* Sets psi (and the heavy-ball previous state psi_old, as the reference does). */
+gpe_status gpe_set_psi(gpe_handle* h, int comp, const double* host_c128);
+gpe_status gpe_get_psi(gpe_handle* h, int comp, double* host_c128);
+gpe_status gpe_set_vext(gpe_handle* h, int comp, const double* host_c128);
+/* Device-resident variants: interleaved complex128 device pointers. */
+gpe_status gpe_set_psi_device(gpe_handle* h, int comp, const void* dev_c128);
+gpe_status gpe_get_psi_device(gpe_handle* h, int comp, void* dev_c128);
+
+/* ---- stepping ---------------------------------------------------------- */
+/* Real-time RK4, OneComponentGPSolver::runRealTimeEvol body
+ * (src/oneComponentGPSolver.cu:150-208) / TwoComponentGPSolver::runRealTimeEvol
+ * (src/twoComponentGPSolver.cu:142-202).  Runs nsteps steps; step j uses the
+ * reference's iteration number first_iteration+j for its stage times
+ * (iteration*dt, (iteration+0.5)*dt, (iteration+1)*dt).  If obs_out is not
+ * NULL, the last step also reduces, per component c, obs_out[3c+0] = sum |psi|^2 DV,
+ * obs_out[3c+1] = sum Re(conj(psi) h_mu) DV and obs_out[3c+2] = sum Re(conj(psi) h_en) DV
+ * pairing the new psi with H of the stage-4 argument, which is what the
+ * reference's status hook reads (hamiltonians/BEC_oneComponent.cu:347-348). */
+gpe_status gpe_step_real(gpe_handle* h, int first_iteration, int nsteps, double* obs_out);
+
+/* Imaginary time (scheme per config).  Heavy-ball: one call runs up to
+ * nsteps iterations of src/oneComponentGPSolver.cu:46-95 (or the 2-component
+ * loop), first_iteration being the reference's `iteration` of the first one.
+ * Stops early at the reference's convergence test; *iters_done counts the
+ * iterations applied (the converging one included), *converged is 1 if the
+ * test fired.  Per-iteration state (E, E_prev, mu, norm) persists across calls. */
+gpe_status gpe_step_imag(gpe_handle* h, int first_iteration, int nsteps,
+                         int* iters_done, int* converged);
+/* PARS after the last imaginary iteration, per component c:
+ * out[4c+0] = NORM, out[4c+1] = MU, out[4c+2] = EN, out[4c+3] = EN_PREV,
+ * with the reference's definitions (1 comp: NORM = npart; 2 comp: NORM is the
+ * pre-renormalisation norm, src/twoComponentGPSolver.cu:64-83). */
+gpe_status gpe_imag_state(gpe_handle* h, double* out);
+/* Resets E, E_prev, mu and the convergence flag (a fresh PARS array). */
+gpe_status gpe_reset_imag_state(gpe_handle* h);
+
+/* ---- primitives -------------------------------------------------------- */
+/* BaseHamiltonian::alg_Laplace (src/baseHamiltonian.cu:86-96): out = IFFT(2pi^2 k^2/N FFT psi_comp). */
+gpe_status gpe_laplace(gpe_handle* h, int comp, double* host_out_c128);
+/* Plugin alg_calcHpsi (both h_mu and h_en) at time t, e.g.
+ * hamiltonians/BEC_oneComponent.cu:92-111; either output may be NULL. */
+gpe_status gpe_apply_h(gpe_handle* h, double t, int comp,
+                       double* host_hmu_c128, double* host_hen_c128);
+/* Raw reductions of the current psi with H(psi) at time t, per component c:
+ * out[3c+0] = sum |psi|^2 DV, out[3c+1] = sum Re(conj(psi) h_mu) DV,
+ * out[3c+2] = sum Re(conj(psi) h_en) DV.  BaseHamiltonian::alg_calcNorm and
+ * alg_calc2Observables (src/baseHamiltonian.cu:173-179,230-236) divide these
+ * by the caller's norm. */
+gpe_status gpe_observables(gpe_handle* h, double t, double* out);
+/* Unnormalised 3D DFT of psi_comp in place, sign -1 (CUFFT_FORWARD) or +1
+ * (CUFFT_INVERSE): the cufftExecZ2Z calls of src/baseHamiltonian.cu:89,95. */
+gpe_status gpe_fft(gpe_handle* h, int comp, int sign);
+
+/* Synchronise the handle's stream and report any asynchronous error. */
+gpe_status gpe_sync(gpe_handle* h);
+/* Number of this library's kernels launched by the handle so far. */
+long long  gpe_kernel_launches(const gpe_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPE_B200_GPE_H */

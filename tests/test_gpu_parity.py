@@ -1,0 +1,213 @@
+"""CUDA path (libgpe.so through the C ABI) against the FP64 host oracle.
+
+Tolerances: complex128 form <= 1e-12 relative (the drop-in bar); complex64
+form (FP32 fields, FP64 reductions) <= 2e-6 relative per primitive.
+"""
+import numpy as np
+import pytest
+
+import oracle_py as orc
+from fgpe_b200 import (C64, C128, HAM_BEC, HAM_BEC2, HAM_DIPOLAR, HAM_TEMPLATE, IMAG_RK4, Solver, grid_axes,
+                       make_config)
+
+from test_oracle import PI_REF, gaussian, harmonic
+
+pytestmark = pytest.mark.gpu
+
+TOL = {C128: 1e-12, C64: 2e-6}
+
+
+def rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300)
+
+
+def pair(cfg, V=None, psi=None, seed=1):
+    g = Solver(cfg)
+    o = orc.OracleSolver(cfg)
+    for c in range(cfg.ncomp):
+        v = harmonic(cfg, (1.0, 1.2, 1.5)) if V is None else V
+        p = gaussian(cfg, seed=seed + c, noise=0.05, npart=cfg.npart[c]) if psi is None else psi
+        g.set_vext(c, v)
+        o.set_vext(c, v)
+        g.set_psi(c, p)
+        o.set_psi(c, p)
+    return g, o
+
+
+SHAPES = [(16, 16, 16), (12, 10, 8), (32, 24, 1), (64, 1, 1), (8, 6, 5), (9, 25, 4), (128, 8, 4)]
+
+
+@pytest.mark.parametrize("prec", [C128, C64])
+@pytest.mark.parametrize("shape", SHAPES)
+def test_fft_forward_inverse(gpu, prec, shape):
+    nx, ny, nz = shape
+    cfg = make_config(shape, 4.0, precision=prec)
+    rng = np.random.default_rng(7)
+    a = rng.standard_normal((nz, ny, nx)) + 1j * rng.standard_normal((nz, ny, nx))
+    with Solver(cfg) as s:
+        s.set_psi(0, a)
+        s.fft(0, -1)
+        f = s.get_psi(0)
+        assert rel(f, np.fft.fftn(a)) < TOL[prec] * 5
+        s.fft(0, +1)
+        assert rel(s.get_psi(0) / a.size, a) < TOL[prec] * 5
+        assert s.launches > 0
+
+
+@pytest.mark.parametrize("prec", [C128, C64])
+@pytest.mark.parametrize("shape", SHAPES)
+def test_laplace(gpu, prec, shape):
+    cfg = make_config(shape, (5.0, 4.0, 3.0), precision=prec, hamiltonian=HAM_TEMPLATE)
+    g, o = pair(cfg)
+    assert rel(g.laplace(0), o.laplace(0)) < TOL[prec]
+
+
+@pytest.mark.parametrize("prec", [C128, C64])
+@pytest.mark.parametrize("shape", [(16, 16, 16), (12, 10, 8), (32, 24, 1)])
+def test_apply_h_and_observables(gpu, prec, shape):
+    prms = np.zeros(32)
+    prms[:6] = [30.0 / (4 * PI_REF), 45.0 / (4 * PI_REF), 40.0 / (4 * PI_REF), 0.01, 0.02, 0.05]
+    cfg = make_config(shape, (5.0, 4.0, 3.0), precision=prec, prms=prms)
+    g, o = pair(cfg)
+    for t in (0.0, 0.005, 0.015, 0.03, 0.1):  # every branch of d_quench_as
+        gm, ge = g.apply_h(t, 0)
+        om, oe = o.apply_h(t, 0)
+        assert rel(gm, om) < TOL[prec]
+        assert rel(ge, oe) < TOL[prec]
+        assert rel(g.observables(t), o.observables(t)) < TOL[prec]
+
+
+@pytest.mark.parametrize("prec", [C128, C64])
+@pytest.mark.parametrize("shape", [(16, 16, 16), (12, 10, 8), (32, 24, 1), (64, 1, 1)])
+def test_real_time_rk4(gpu, prec, shape):
+    prms = np.zeros(32)
+    prms[:6] = [30.0 / (4 * PI_REF), 33.0 / (4 * PI_REF), 33.0 / (4 * PI_REF), 0.0, 1e300, 1e300]
+    cfg = make_config(shape, (5.0, 4.0, 3.0), dt=1e-3, precision=prec, prms=prms)
+    g, o = pair(cfg)
+    og = g.step_real(0, 20, want_obs=True)
+    oo = o.step_real(0, 20, want_obs=True)
+    tol = TOL[prec] if prec == C128 else 1e-5
+    assert rel(g.get_psi(0), o.get_psi(0)) < tol
+    assert rel(og, oo) < tol
+    # a second chunk continues the reference's iteration count
+    g.step_real(20, 5)
+    o.step_real(20, 5)
+    assert rel(g.get_psi(0), o.get_psi(0)) < tol
+
+
+@pytest.mark.parametrize("prec", [C128, C64])
+@pytest.mark.parametrize("shape", [(16, 16, 16), (12, 10, 8), (32, 24, 1), (64, 1, 1)])
+def test_imag_heavyball(gpu, prec, shape):
+    cfg = make_config(shape, (5.0, 4.0, 3.0), dt=2e-3, precision=prec, g=25.0, beta=0.9, epsilon_e=0.0)
+    g, o = pair(cfg)
+    dg = g.step_imag(0, 30)
+    do = o.step_imag(0, 30)
+    assert dg == do == (30, False)
+    tol = TOL[prec] if prec == C128 else 1e-5
+    assert rel(g.get_psi(0), o.get_psi(0)) < tol
+    sg, so = g.imag_state(), o.imag_state()
+    assert np.allclose(sg, so, rtol=tol, atol=0)
+    # continue after get_psi materialised the lazy normalisation
+    g.step_imag(30, 10)
+    o.step_imag(30, 10)
+    assert rel(g.get_psi(0), o.get_psi(0)) < tol
+    assert np.allclose(g.imag_state(), o.imag_state(), rtol=tol, atol=0)
+
+
+def test_imag_heavyball_convergence_iteration(gpu):
+    # The device-side convergence test must stop at the same iteration as the
+    # reference loop (|dE|/E_prev < eps, src/oneComponentGPSolver.cu:84).
+    cfg = make_config((16, 16, 16), 6.0, dt=5e-3, g=10.0, beta=0.5, epsilon_e=1e-7)
+    g, o = pair(cfg)
+    dg = g.step_imag(0, 2000)
+    do = o.step_imag(0, 2000)
+    assert dg == do and dg[1]
+    assert rel(g.get_psi(0), o.get_psi(0)) < 1e-12
+
+
+@pytest.mark.parametrize("prec", [C128, C64])
+def test_imag_rk4(gpu, prec):
+    cfg = make_config((16, 16, 16), 6.0, dt=5e-3, g=10.0, precision=prec, imag_scheme=IMAG_RK4, epsilon_e=0.0)
+    g, o = pair(cfg)
+    assert g.step_imag(0, 25) == o.step_imag(0, 25)
+    tol = TOL[prec] if prec == C128 else 1e-5
+    assert rel(g.get_psi(0), o.get_psi(0)) < tol
+    assert np.allclose(g.imag_state(), o.imag_state(), rtol=tol, atol=0)
+
+
+@pytest.mark.parametrize("prec", [C128, C64])
+@pytest.mark.parametrize("shape", [(16, 12, 8), (24, 24, 1)])
+def test_two_component(gpu, prec, shape):
+    prms = [30.0 / (4 * PI_REF), 28.5 / (4 * PI_REF), 27.0 / (4 * PI_REF)]
+    cfg = make_config(shape, (5.0, 4.0, 3.0), dt=1e-3, ncomp=2, hamiltonian=HAM_BEC2, prms=prms,
+                      npart=(0.5, 0.5), beta=0.5, precision=prec)
+    V = harmonic(cfg) + 0.1j * harmonic(cfg)  # complex V exercises the vext1.y quirk
+    g, o = pair(cfg, V=V)
+    tol = TOL[prec] if prec == C128 else 1e-5
+    for c in range(2):
+        assert rel(g.apply_h(0.0, c)[1], o.apply_h(0.0, c)[1]) < TOL[prec]
+    assert g.step_imag(0, 15) == o.step_imag(0, 15)
+    for c in range(2):
+        assert rel(g.get_psi(c), o.get_psi(c)) < tol
+    assert np.allclose(g.imag_state(), o.imag_state(), rtol=tol, atol=0)
+    g.step_real(0, 10)
+    o.step_real(0, 10)
+    for c in range(2):
+        assert rel(g.get_psi(c), o.get_psi(c)) < tol
+
+
+@pytest.mark.parametrize("prec", [C128, C64])
+def test_dipolar(gpu, prec):
+    prms = np.zeros(32)
+    a = 40.0 / (4 * PI_REF)
+    prms[:3] = a
+    prms[6] = 0.8 * a
+    prms[7:10] = [0.0, 0.0, 1.0]
+    prms[10] = 3.0
+    cfg = make_config((16, 16, 8), (6.0, 6.0, 3.0), dt=1e-3, precision=prec, prms=prms,
+                      hamiltonian=HAM_DIPOLAR, beta=0.5)
+    g, o = pair(cfg)
+    for c_ in (0,):
+        gm, ge = g.apply_h(0.0, c_)
+        om, oe = o.apply_h(0.0, c_)
+        assert rel(gm, om) < TOL[prec] * 2
+        assert rel(ge, oe) < TOL[prec] * 2
+    tol = TOL[prec] if prec == C128 else 1e-5
+    g.step_imag(0, 10)
+    o.step_imag(0, 10)
+    assert rel(g.get_psi(0), o.get_psi(0)) < tol
+    g.step_real(0, 10)
+    o.step_real(0, 10)
+    assert rel(g.get_psi(0), o.get_psi(0)) < tol
+
+
+def test_template_hamiltonian(gpu):
+    cfg = make_config((16, 16, 16), 5.0, dt=1e-3, hamiltonian=HAM_TEMPLATE)
+    g, o = pair(cfg)
+    gm, ge = g.apply_h(0.0, 0)
+    om, oe = o.apply_h(0.0, 0)
+    assert rel(gm, om) < 1e-12 and rel(ge, oe) < 1e-12
+    g.step_real(0, 10)
+    o.step_real(0, 10)
+    assert rel(g.get_psi(0), o.get_psi(0)) < 1e-12
+
+
+def test_diverged_watchdog(gpu):
+    # NaN injected into psi on the host: the device watchdog reports GPE_ERR_DIVERGED.
+    from fgpe_b200 import GPEError
+    cfg = make_config((16, 16, 16), 5.0, dt=1e-3, g=10.0, beta=0.5)
+    s = Solver(cfg)
+    p = gaussian(cfg)
+    p[3, 4, 5] = np.nan
+    s.set_vext(0, harmonic(cfg))
+    s.set_psi(0, p)
+    with pytest.raises(GPEError) as e:
+        s.step_imag(0, 5)
+    assert e.value.status == 5
+
+
+def test_unsupported_length_rejected(gpu):
+    from fgpe_b200 import GPEError
+    with pytest.raises(GPEError) as e:
+        Solver(make_config((14, 8, 8), 4.0))
+    assert e.value.status == 2
