@@ -1,0 +1,424 @@
+#!/usr/bin/env python3
+"""bench.py -- RK4 steps/s of the GPE real-time hot path on B200.
+
+Workload (the headline configuration): single-component real-time quench on a
+128^3 grid over [-10,10]^3 in oscillator units, V = 0.5(x^2 + y^2 + (2z)^2),
+starting from the imaginary-time ground state at g = 1000 computed in the same
+run (heavy-ball scheme of the reference), then g -> 1100 at t = 0 and RK4 with
+dt = 5e-4.  The measured form is complex64 fields/FFTs with FP64 stage
+coefficients and FP64 compensated reductions; the plain complex128 drop-in is
+timed beside it, and the accuracy of the complex64 form after 10^4 steps is
+reported against complex128 (pinned to the FP64 oracle by the test suite).
+
+One "step" = one full RK4 step (4 stages x 5 fused axis passes).  L2 is
+flushed (256 MiB write) before every timed step; each step is bracketed by
+CUDA events on the library's stream.  `--impl reference` times the FP64 host
+oracle port of the reference's algorithm (the reference has no CPU path).
+Multi-GPU: the path does not shard (replicas only); every rank runs its own
+instance and value = total steps / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_GRID = 128
+L_BOX = 10.0
+G0, G1 = 1000.0, 1100.0
+DT = 5e-4
+PI_REF = 3.141592653589793
+F_PER_STEP_KERNELS = {"x_fwd": 2.0, "x_inv": 6.25, "s_fwd": 2.0, "s_inv": 2.0, "s_fki": 2.0, "x_full": 0.0}
+# Algorithmic field transfers per launch of each pass kind in the 1-component
+# real-time RK4 step (F = one field): x-forward reads the stage state and
+# writes the work field; strided passes read and write the work field;
+# x-inverse epilogue stage 1/2/3/4 moves 5/7/7/6 fields (mean 6.25).
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--accuracy-steps", type=int, default=10000)
+    p.add_argument("--quick", action="store_true", help="skip the 10^4-step accuracy run and the CPU baseline")
+    p.add_argument("--grid", type=int, default=N_GRID)
+    p.add_argument("--ground-steps", type=int, default=3000, help="heavy-ball iterations for the initial state")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def workload_config(n, precision, g, imag=False):
+    import fgpe_b200 as gp
+    prms = np.zeros(32)
+    prms[0:3] = g / (4 * PI_REF)
+    return gp.make_config((n, n, n), L_BOX, dt=(2e-3 if imag else DT), precision=precision, prms=prms,
+                          beta=0.9, npart=(1.0, 1.0), epsilon_e=1e-12)
+
+
+def trap(cfg):
+    import fgpe_b200 as gp
+    x, y, z = gp.grid_axes(cfg)
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    return 0.5 * (X ** 2 + Y ** 2 + (2 * Z) ** 2) + 0j
+
+
+def initial_psi(cfg, seed=1):
+    import fgpe_b200 as gp
+    x, y, z = gp.grid_axes(cfg)
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    rng = np.random.default_rng(seed)
+    g = np.exp(-(X ** 2 + Y ** 2 + Z ** 2) / 2.0)
+    psi = g * (1 + 1e-3 * (rng.standard_normal(g.shape) + 1j * rng.standard_normal(g.shape)))
+    dv = cfg.dx[0] * cfg.dx[1] * cfg.dx[2]
+    return psi / np.sqrt(np.sum(np.abs(psi) ** 2) * dv)
+
+
+def ground_state(n, stream_ptr, iters=3000):
+    """Heavy-ball imaginary time (the reference's scheme) at g = 1000, complex128."""
+    import fgpe_b200 as gp
+    cfg = workload_config(n, gp.C128, G0, imag=True)
+    s = gp.Solver(cfg)
+    s.set_stream(stream_ptr)
+    s.set_vext(0, trap(cfg))
+    s.set_psi(0, initial_psi(cfg))
+    done, conv = s.step_imag(0, iters)
+    st = s.imag_state()
+    psi = s.get_psi(0)
+    s.close()
+    return psi, {"iterations": done, "converged": bool(conv), "mu": float(st[1]), "E": float(st[2])}
+
+
+class Clocks:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"gpe_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        if not self.proc or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        top = sorted(sm)[len(sm) // 2:] if len(sm) > 4 else sm  # samples under load
+        return {"sm_mhz": float(np.median(top)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def time_steps(solver, torch, flush, steps, first_it, profile=False):
+    """K RK4 steps, L2 flushed before each, CUDA events on the library stream."""
+    st = torch.cuda.current_stream()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    solver.profile(profile)
+    if profile:
+        solver.profile_read()
+    l0 = solver.launches
+    for k in range(steps):
+        flush.zero_()
+        evs[k][0].record(st)
+        solver.step_real(first_it + k, 1)
+        evs[k][1].record(st)
+    torch.cuda.synchronize()
+    launches = solver.launches - l0
+    ms = float(sum(a.elapsed_time(b) for a, b in evs))
+    prof = solver.profile_read() if profile else None
+    solver.profile(False)
+    return ms, launches, prof
+
+
+def run_ours(args):
+    import torch
+    import fgpe_b200 as gp
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    stream_ptr = torch.cuda.current_stream().cuda_stream
+    n = args.grid
+    K, W = args.steps, max(args.warmup, 3)
+
+    psi_gs, prep = ground_state(n, stream_ptr, args.ground_steps)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    solvers = {}
+    for name, prec in (("c64", gp.C64), ("c128", gp.C128)):
+        cfg = workload_config(n, prec, G1)
+        s = gp.Solver(cfg)
+        s.set_stream(stream_ptr)
+        s.set_vext(0, trap(cfg))
+        s.set_psi(0, psi_gs)
+        solvers[name] = s
+
+    results = {}
+    with Clocks(dev) as clk:
+        for name, s in solvers.items():
+            for w in range(W):
+                flush.zero_()
+                s.step_real(w, 1)
+            torch.cuda.synchronize()
+            ms, launches, _ = time_steps(s, torch, flush, K, W)
+            ms_p, _, prof = time_steps(s, torch, flush, K, W + K, profile=True)
+            results[name] = {"ms": ms, "launches": launches, "ms_prof": ms_p, "prof": prof}
+    clocks = clk.summary()
+
+    # max over ranks
+    ms64, ms128 = results["c64"]["ms"], results["c128"]["ms"]
+    if dist is not None:
+        t = torch.tensor([ms64, ms128], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms64, ms128 = float(t[0]), float(t[1])
+        dist.barrier()
+    if rank != 0:
+        for s in solvers.values():
+            s.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    N = n ** 3
+    F64 = 8 * N  # one complex64 field in bytes
+    value = world * K / (ms64 / 1e3)
+    value128 = world * K / (ms128 / 1e3)
+
+    # roofline of the dominant pass kernel (complex64 form), live event timing
+    prof = results["c64"]["prof"]
+    dom = max((k for k in prof if prof[k][1] > 0), key=lambda k: prof[k][0])
+    dom_ms, dom_cnt = prof[dom]
+    dom_bytes = F_PER_STEP_KERNELS[dom] * F64
+    achieved = dom_bytes / (dom_ms / dom_cnt / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic_128cubed_c64.txt")
+    if os.path.exists(tpath):
+        for line in open(tpath):
+            f = line.split()
+            if len(f) >= 2 and f[0] == dom:
+                traffic = float(f[1])
+    step_bytes = sum(F_PER_STEP_KERNELS[k] * F64 * prof[k][1] for k in prof) / K
+    step_ms = ms64 / K
+
+    # e2e through the C ABI: H2D of the step's psi (pinned, complex128) + 1 step + D2H of observables
+    import torch as _t
+    s = solvers["c64"]
+    host = _t.empty(2 * N, dtype=_t.float64, pin_memory=True)
+    hv = host.numpy().view(np.complex128)
+    hv[:] = psi_gs.reshape(-1)
+    e2e_t = []
+    for k in range(W + K):
+        t0 = time.perf_counter()
+        s.set_psi(0, hv)
+        s.step_real(k, 1, want_obs=True)
+        t1 = time.perf_counter()
+        if k >= W:
+            e2e_t.append(t1 - t0)
+    e2e = {"value": world * K / sum(e2e_t), "unit": "steps/s", "h2d_bytes_per_step": 16 * N,
+           "d2h_bytes_per_step": 208, "note": "gpe_set_psi(host pinned complex128) + gpe_step_real(1, observables)"}
+
+    line = {
+        "metric": "RK4 steps/s at 128^3 (complex64 + FP64 reductions, real-time quench)",
+        "value": round(value, 2),
+        "unit": "steps/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": round(step_ms, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded Gaussian -> heavy-ball ground state at g=1000, quench to g=1100)",
+        "config": {"workload": f"real-time RK4 quench, {n}^3 on [-10,10]^3, V=0.5(x^2+y^2+4z^2), "
+                               f"g 1000->1100, dt 5e-4",
+                   "grid": [n, n, n], "form": "complex64 fields/FFT, FP64 stage coefficients and reductions",
+                   "l2": "flushed before every timed step (256 MiB write)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "plain_c128": {"value": round(value128, 2), "unit": "steps/s", "ms_per_step": round(ms128 / K, 5),
+                       "speedup_c64_over_c128": round(value / value128, 3)},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes,
+                     "step_algorithmic_bytes": step_bytes,
+                     "step_achieved_gbs": round(step_bytes / (step_ms / 1e3) / 1e9, 1),
+                     "step_frac": round(step_bytes / (step_ms / 1e3) / 1e9 / peak, 4),
+                     "survey_45F_step_frac": round(45 * F64 / (step_ms / 1e3) / 1e9 / peak, 4),
+                     "per_kind_ms_per_launch": {k: round(v[0] / v[1], 5) for k, v in prof.items() if v[1]},
+                     "profiled_ms_per_step": round(results["c64"]["ms_prof"] / K, 5)},
+        "e2e": e2e,
+        "gpu_launches": results["c64"]["launches"],
+        "clocks": clocks,
+        "prep": prep,
+    }
+
+    if not args.quick:
+        line["accuracy"] = accuracy(solvers, psi_gs, args.accuracy_steps)
+        line["cpu_baseline"] = cpu_baseline(n)
+    else:
+        line["cpu_baseline"] = None
+    for s2 in solvers.values():
+        s2.close()
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def accuracy(solvers, psi_gs, nsteps):
+    """complex64 vs complex128 after nsteps RK4 steps from the same ground state."""
+    out = {"steps": nsteps}
+    res = {}
+    for name, s in solvers.items():
+        s.set_psi(0, psi_gs)
+        o0 = s.observables(0.0)
+        chunk = 500
+        for k in range(0, nsteps, chunk):
+            s.step_real(k, min(chunk, nsteps - k))
+        o1 = s.observables(nsteps * DT)
+        res[name] = (s.get_psi(0), o0, o1)
+    p64, a0, a1 = res["c64"]
+    p128, b0, b1 = res["c128"]
+    out["psi_rel_l2_c64_vs_c128"] = float(np.linalg.norm(p64 - p128) / np.linalg.norm(p128))
+    norm = b1[0]
+    out["E_rel_err"] = float(abs(a1[2] / a1[0] - b1[2] / b1[0]) / abs(b1[2] / b1[0]))
+    out["mu_rel_err"] = float(abs(a1[1] / a1[0] - b1[1] / b1[0]) / abs(b1[1] / b1[0]))
+    out["norm_drift_c64"] = float(a1[0] / a0[0] - 1)
+    out["norm_drift_c128"] = float(b1[0] / b0[0] - 1)
+    out["energy_drift_c64"] = float(a1[2] / a0[2] - 1)
+    out["energy_drift_c128"] = float(b1[2] / b0[2] - 1)
+    out["E_c128"] = float(b1[2] / norm)
+    out["reference_for_error"] = "complex128 path (parity-tested against the FP64 oracle at <= 1e-12)"
+    return out
+
+
+def cpu_baseline(n, budget_s=12.0):
+    """FP64 oracle port of the reference algorithm on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as orc
+    import fgpe_b200 as gp
+    threads = os.cpu_count() or 1
+    orc.set_threads(threads)
+    cfg = workload_config(n, gp.C128, G1)
+    o = orc.OracleSolver(cfg)
+    o.set_vext(0, trap(cfg))
+    o.set_psi(0, initial_psi(cfg))
+    t0 = time.perf_counter()
+    o.step_real(0, 1)
+    one = time.perf_counter() - t0
+    k = max(1, int(budget_s / max(one, 1e-3)))
+    t0 = time.perf_counter()
+    o.step_real(1, k)
+    dt = time.perf_counter() - t0
+    o.close()
+    return {"value": round(k / dt, 4), "unit": "steps/s", "cores": threads, "kind": "port",
+            "sample": f"{k} RK4 steps of the same {n}^3 workload in FP64 (oracle/gpe_oracle.cpp, OpenMP)"}
+
+
+def run_reference(args):
+    """CPU reference arm: the oracle port (the reference has no CPU path)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as orc
+    import fgpe_b200 as gp
+    threads = os.cpu_count() or 1
+    orc.set_threads(threads)
+    n = args.grid
+    cfg = workload_config(n, gp.C128, G1)
+    o = orc.OracleSolver(cfg)
+    o.set_vext(0, trap(cfg))
+    o.set_psi(0, initial_psi(cfg))
+    W, K = max(args.warmup, 1), args.steps
+    # bounded sample: at most ~60 s of timed CPU work
+    t0 = time.perf_counter()
+    o.step_real(0, 1)
+    one = time.perf_counter() - t0
+    K = max(1, min(K, int(60.0 / max(one, 1e-3))))
+    W = min(W, 2)
+    o.step_real(1, W - 1) if W > 1 else None
+    t0 = time.perf_counter()
+    o.step_real(W, K)
+    dt = time.perf_counter() - t0
+    v = K / dt
+    line = {"impl": "reference", "metric": "RK4 steps/s at 128^3 (complex64 + FP64 reductions, real-time quench)",
+            "value": round(v, 4), "unit": "steps/s", "n_gpus": 1, "steps": K, "warmup": W,
+            "ms_per_step": round(1e3 * dt / K, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"real-time RK4 quench, {n}^3 on [-10,10]^3, V=0.5(x^2+y^2+4z^2), "
+                                   f"g 1000->1100, dt 5e-4", "grid": [n, n, n]},
+            "cpu_baseline": {"value": round(v, 4), "unit": "steps/s", "cores": threads, "kind": "port",
+                             "sample": f"{K} FP64 RK4 steps (oracle port of the reference algorithm; "
+                                       f"the reference has no CPU path)"},
+            "e2e": {"value": round(v, 4), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -97,6 +97,8 @@ def lib() -> ctypes.CDLL:
         "gpe_fft": (c_int, [H, c_int, c_int]),
         "gpe_sync": (c_int, [H]),
         "gpe_kernel_launches": (c_longlong, [H]),
+        "gpe_profile_enable": (c_int, [H, c_int]),
+        "gpe_profile_read": (c_int, [H, P, POINTER(c_longlong)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -275,3 +277,15 @@ class Solver:
     @property
     def launches(self) -> int:
         return int(lib().gpe_kernel_launches(self._h))
+
+    PROF_KINDS = ("x_fwd", "x_inv", "x_full", "s_fwd", "s_inv", "s_fki")
+
+    def profile(self, enable: bool) -> None:
+        _check(lib().gpe_profile_enable(self._h, 1 if enable else 0))
+
+    def profile_read(self) -> dict:
+        """{kind: (summed ms, launches)} since the previous read (syncs)."""
+        ms = np.zeros(len(self.PROF_KINDS))
+        cnt = (c_longlong * len(self.PROF_KINDS))()
+        _check(lib().gpe_profile_read(self._h, _dp(ms), cnt))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.PROF_KINDS)}

@@ -74,6 +74,14 @@ struct gpe_handle {
     long long launches = 0;
     int mode = ST_CANON;
     bool hb_old_valid = true;
+    // per-pass event timing (gpe_profile_enable)
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_free;
+    struct Rec {
+        int kind;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> recs;
 };
 
 // ---- small element-wise kernels ------------------------------------------------------
@@ -229,13 +237,148 @@ PassArgs<R> base_args(gpe_handle* h) {
     return a;
 }
 
+cudaEvent_t take_event(gpe_handle* h) {
+    if (!h->ev_free.empty()) {
+        cudaEvent_t e = h->ev_free.back();
+        h->ev_free.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Brackets one launch with events when profiling is on.
+struct ProfScope {
+    gpe_handle* h;
+    int kind;
+    cudaEvent_t a = nullptr;
+    ProfScope(gpe_handle* h_, int kind_) : h(h_), kind(kind_) {
+        if (h->prof) {
+            a = take_event(h);
+            cudaEventRecord(a, h->st);
+        }
+    }
+    ~ProfScope() {
+        if (a) {
+            cudaEvent_t b = take_event(h);
+            cudaEventRecord(b, h->st);
+            h->recs.push_back(gpe_handle::Rec{kind, a, b});
+        }
+    }
+};
+
+int prof_kind(int mode) {
+    switch (mode) {
+        case XM_FWD: return 0;
+        case XM_INV: return 1;
+        case XM_FULL: return 2;
+        case SM_FWD: return 3;
+        case SM_INV: return 4;
+        default: return 5;
+    }
+}
+
+// Shared-memory budget of one pass CTA (staged slots + FFT exchange buffer).
+constexpr size_t SMEM_BUDGET = 96 * 1024;
+
+template <typename R>
+struct Stager {
+    typedef typename Cx<R>::T C;
+    PassArgs<R>& a;
+    explicit Stager(PassArgs<R>& a_) : a(a_) {
+        a.nstage = 0;
+        for (int i = 0; i < 3; ++i) a.s_w[i] = -1;
+        for (int i = 0; i < 2; ++i) a.s_psi[i] = a.s_v[i] = a.s_a[i] = a.s_k[i] = a.s_xo[i] = -1;
+    }
+    int add(const C* p, int kind, int comp) {
+        const int s = a.nstage++;
+        a.stage_ptr[s] = p;
+        a.stage_kind[s] = kind;
+        a.stage_comp[s] = comp;
+        return s;
+    }
+    // psi source of the prologue / epilogue per a.pro
+    void psi(int npsi) {
+        for (int c = 0; c < npsi; ++c) {
+            if (a.s_psi[c] >= 0) continue;
+            if (a.pro == PRO_PIN) a.s_psi[c] = add(a.pin[c], SK_FIXED, c);
+            else if (a.pro == PRO_CUR) a.s_psi[c] = add(nullptr, SK_CUR, c);
+            else a.s_psi[c] = add(a.buf[0][c], SK_FIXED, c);
+        }
+    }
+    // Fields read by the epilogue op (see epilogue_point).
+    void epilogue(int npsi) {
+        switch (a.epi) {
+            case EPI_STORE:
+                return;
+            case EPI_RK:
+                psi(npsi);
+                for (int c = 0; c < npsi; ++c) {
+                    a.s_v[c] = add(a.vext[c], SK_FIXED, c);
+                    if (a.stage > 1) {
+                        a.s_a[c] = add(a.buf[0][c], SK_FIXED, c);
+                        a.s_k[c] = add(a.kacc[c], SK_FIXED, c);
+                    }
+                }
+                return;
+            case EPI_HB:
+                psi(npsi);
+                for (int c = 0; c < npsi; ++c) {
+                    a.s_xo[c] = add(nullptr, SK_OLD, c);
+                    a.s_v[c] = add(a.vext[c], SK_FIXED, c);
+                }
+                return;
+            case EPI_RKI:
+                for (int c = 0; c < npsi; ++c) {
+                    if (a.stage == 1 && a.pro == PRO_A_SCALED) {
+                        psi(npsi);
+                        a.s_a[c] = a.s_psi[c];
+                    } else {
+                        a.s_a[c] = add(a.buf[0][c], SK_FIXED, c);
+                        if (a.stage > 1) {
+                            if (a.s_psi[c] < 0) a.s_psi[c] = add(a.pin[c], SK_FIXED, c);
+                            a.s_k[c] = add(a.kacc[c], SK_FIXED, c);
+                        }
+                    }
+                    a.s_v[c] = add(a.vext[c], SK_FIXED, c);
+                }
+                return;
+            default:  // EPI_APPLYH, EPI_OBS
+                psi(npsi);
+                for (int c = 0; c < npsi; ++c) a.s_v[c] = add(a.vext[c], SK_FIXED, c);
+                return;
+        }
+    }
+};
+
 template <typename R>
 gpe_status launch_x(gpe_handle* h, PassArgs<R> a, int nf, int mode) {
+    typedef typename Cx<R>::T C;
+    ProfScope ps(h, prof_kind(mode));
     a.mode = mode;
-    a.tw = (const typename Cx<R>::T*)h->tw[0];
+    a.tw = (const C*)h->tw[0];
+    const int npsi = nf - a.dens;
+    Stager<R> sg(a);
+    if (mode == XM_FWD || mode == XM_FULL) sg.psi(npsi);
+    if (mode == XM_INV)
+        for (int f = 0; f < nf; ++f) a.s_w[f] = sg.add(a.w[f], SK_FIXED, f);
+    if (mode == XM_INV || mode == XM_FULL) sg.epilogue(npsi);
+    const int L = h->nx;
+    // 2 staging buffers + padded exchange buffers (one per field: the
+    // inverse results of all fields meet in the epilogue)
+    const size_t row_bytes = ((size_t)2 * a.nstage * L + (size_t)nf * xpad(L)) * sizeof(C);
+    const int T = plan_T(L);
+    const int bmax = (256 / T) > 0 ? 256 / T : 1;
+    int rows = (int)(SMEM_BUDGET / row_bytes);
+    if (rows > bmax) rows = bmax;
+    if (rows < 1) rows = 1;
+    if ((size_t)rows * row_bytes > 220 * 1024)
+        return fail(GPE_ERR_UNSUPPORTED, "x-pass tile does not fit in shared memory (length " + std::to_string(L) + ")");
+    a.tma = ((size_t)L * sizeof(C)) % 16 == 0 ? 1 : 0;
     cudaError_t err = cudaSuccess;
-    if (!dispatch_x(h->nx, nf, a, h->st, &err))
-        return fail(GPE_ERR_UNSUPPORTED, "no x-pass kernel for length " + std::to_string(h->nx));
+    if (!dispatch_x(L, nf, a, rows, (size_t)rows * row_bytes, h->st, &err))
+        return fail(GPE_ERR_UNSUPPORTED, "no x-pass kernel for length " + std::to_string(L));
     if (err != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("x pass launch: ") + cudaGetErrorString(err));
     h->launches++;
     return GPE_OK;
@@ -243,14 +386,19 @@ gpe_status launch_x(gpe_handle* h, PassArgs<R> a, int nf, int mode) {
 
 template <typename R>
 gpe_status launch_s(gpe_handle* h, PassArgs<R> a, int nf, int axis, int mode) {
+    typedef typename Cx<R>::T C;
+    ProfScope ps(h, prof_kind(mode));
     const int L = axis == 1 ? h->ny : h->nz;
     const int T = plan_T(L);
     int tx = h->nx < 16 ? h->nx : 16;
     while (tx > 1 && tx * T > 512) tx /= 2;
+    while (tx > 1 && (size_t)(2 * nf + 1) * L * tx * sizeof(C) > SMEM_BUDGET) tx /= 2;
     a.mode = mode;
     a.sax = axis;
     a.tx = tx;
-    a.tw = (const typename Cx<R>::T*)h->tw[axis];
+    a.tw = (const C*)h->tw[axis];
+    Stager<R> sg(a);
+    for (int f = 0; f < nf; ++f) a.s_w[f] = sg.add(a.w[f], SK_FIXED, f);
     int nouter;
     if (axis == 1) {
         a.sstride = h->nx;
@@ -261,8 +409,11 @@ gpe_status launch_s(gpe_handle* h, PassArgs<R> a, int nf, int axis, int mode) {
         a.ostride = h->nx;
         nouter = h->ny;
     }
+    const size_t es = sizeof(C);
+    a.tma = ((h->nx * es) % 16 == 0 && (tx * es) % 16 == 0 && ((h->nx % tx) * es) % 16 == 0) ? 1 : 0;
+    const size_t smem = (size_t)(2 * nf + 1) * L * tx * es;
     cudaError_t err = cudaSuccess;
-    if (!dispatch_s(L, nf, a, nouter, h->st, &err))
+    if (!dispatch_s(L, nf, a, nouter, smem, h->st, &err))
         return fail(GPE_ERR_UNSUPPORTED, "no strided-pass kernel for length " + std::to_string(L));
     if (err != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("strided pass launch: ") + cudaGetErrorString(err));
     h->launches++;
@@ -288,6 +439,16 @@ gpe_status run_chain(gpe_handle* h, const PassArgs<R>& a, int nf) {
 gpe_status sync_read_scalars(gpe_handle* h, DevScalars* out) {
     GPE_CUDA(cudaMemcpyAsync(out, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->st));
     GPE_CUDA(cudaStreamSynchronize(h->st));
+    return GPE_OK;
+}
+
+// Synchronise and report a device-side error recorded by a kernel (bounded
+// wait expired, non-finite reduction).
+gpe_status check_device_status(gpe_handle* h) {
+    DevScalars s;
+    GPE_TRY(sync_read_scalars(h, &s));
+    if (s.status == GPE_ERR_TIMEOUT) return fail(GPE_ERR_TIMEOUT, "a bounded device wait expired");
+    if (s.status == GPE_ERR_DIVERGED) return fail(GPE_ERR_DIVERGED, "non-finite norm, energy or chemical potential");
     return GPE_OK;
 }
 
@@ -348,6 +509,8 @@ gpe_status step_real_t(gpe_handle* h, int first, int nsteps, double* obs_out) {
         DevScalars s;
         GPE_TRY(sync_read_scalars(h, &s));
         for (int q = 0; q < 3 * h->ncomp; ++q) obs_out[q] = s.obs[q];
+        if (s.status == GPE_ERR_TIMEOUT) return fail(GPE_ERR_TIMEOUT, "a bounded device wait expired");
+        if (s.status == GPE_ERR_DIVERGED) return fail(GPE_ERR_DIVERGED, "non-finite observable");
     }
     return GPE_OK;
 }
@@ -399,16 +562,19 @@ gpe_status step_imag_t(gpe_handle* h, int first, int nsteps, int* iters_done, in
     if (iters_done) *iters_done = s.iters_done;
     if (converged) *converged = s.converged;
     if (s.status == GPE_ERR_DIVERGED) return fail(GPE_ERR_DIVERGED, "non-finite norm, energy or chemical potential");
+    if (s.status == GPE_ERR_TIMEOUT) return fail(GPE_ERR_TIMEOUT, "a bounded device wait expired");
     return GPE_OK;
 }
 
 template <typename R>
-gpe_status apply_chain_t(gpe_handle* h, int epi, double t, int comp_only) {
+gpe_status apply_chain_t(gpe_handle* h, int epi, double t, int comp_only, int spec = SPEC_KIN) {
     GPE_TRY(canonicalize_t<R>(h));
     PassArgs<R> a = base_args<R>(h);
     a.pro = PRO_PIN;
     a.epi = epi;
     a.t = t;
+    a.spec = spec;
+    if (spec == SPEC_PX) a.ham = GPE_HAM_TEMPLATE;
     int nf = h->nf;
     if (comp_only >= 0) {  // single component, kinetic only (Laplace / FFT tools)
         a.ncomp = 1;
@@ -504,6 +670,11 @@ void free_all(gpe_handle* h) {
                     h->kax[1], h->kax[2], h->vdd, h->prms, h->sc, h->partials, h->stage128};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    for (auto& r : h->recs) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (auto e : h->ev_free) cudaEventDestroy(e);
 }
 
 }  // namespace
@@ -647,8 +818,7 @@ gpe_status gpe_create(const gpe_config* cfg, gpe_handle** out) {
         s.norm[1] = cfg->npart[1];
         cudaMemcpy(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice);
     }
-    const int B = 256 / plan_T(h->nx) > 0 ? 256 / plan_T(h->nx) : 1;
-    const size_t nblk = (size_t)(h->ny * h->nz + B - 1) / B;
+    const size_t nblk = (size_t)h->ny * h->nz;  // x-pass CTAs hold >= 1 row each
     if (!dmalloc((void**)&h->partials, nblk * MAXQ * 2 * sizeof(double))) return bail(GPE_ERR_OUT_OF_MEMORY);
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
@@ -796,6 +966,7 @@ gpe_status gpe_laplace(gpe_handle* h, int comp, double* host_out_c128) {
     if (!host_out_c128) return fail(GPE_ERR_INVALID_ARG, "null output");
     GPE_TRY(h->prec == GPE_C64 ? apply_chain_t<float>(h, EPI_STORE, 0.0, comp)
                                : apply_chain_t<double>(h, EPI_STORE, 0.0, comp));
+    GPE_TRY(check_device_status(h));
     return download_c128_host(h, h->W[0], host_out_c128);
 }
 
@@ -805,6 +976,7 @@ gpe_status gpe_apply_h(gpe_handle* h, double t, int comp, double* hmu, double* h
     GPE_TRY(ensure_out_buffers(h));
     GPE_TRY(h->prec == GPE_C64 ? apply_chain_t<float>(h, EPI_APPLYH, t, -1)
                                : apply_chain_t<double>(h, EPI_APPLYH, t, -1));
+    GPE_TRY(check_device_status(h));
     if (hmu) GPE_TRY(download_c128_host(h, h->O[2 * comp], hmu));
     if (hen) GPE_TRY(download_c128_host(h, h->O[2 * comp + 1], hen));
     return GPE_OK;
@@ -821,20 +993,60 @@ gpe_status gpe_observables(gpe_handle* h, double t, double* out) {
     return GPE_OK;
 }
 
+gpe_status gpe_momentum_x(gpe_handle* h, int comp, double* px) {
+    GPE_TRY(check_handle(h));
+    GPE_TRY(check_comp(h, comp));
+    if (!px) return fail(GPE_ERR_INVALID_ARG, "null output");
+    GPE_TRY(h->prec == GPE_C64 ? apply_chain_t<float>(h, EPI_OBS, 0.0, comp, SPEC_PX)
+                               : apply_chain_t<double>(h, EPI_OBS, 0.0, comp, SPEC_PX));
+    DevScalars s;
+    GPE_TRY(sync_read_scalars(h, &s));
+    *px = s.obs[1];
+    return GPE_OK;
+}
+
 gpe_status gpe_fft(gpe_handle* h, int comp, int sign) {
     GPE_TRY(check_handle(h));
     GPE_TRY(check_comp(h, comp));
     if (sign != -1 && sign != 1) return fail(GPE_ERR_INVALID_ARG, "sign must be -1 or +1");
-    return h->prec == GPE_C64 ? fft_t<float>(h, comp, sign) : fft_t<double>(h, comp, sign);
+    GPE_TRY(h->prec == GPE_C64 ? fft_t<float>(h, comp, sign) : fft_t<double>(h, comp, sign));
+    return check_device_status(h);
 }
 
 gpe_status gpe_sync(gpe_handle* h) {
     GPE_TRY(check_handle(h));
     GPE_CUDA(cudaStreamSynchronize(h->st));
     GPE_CUDA(cudaGetLastError());
-    return GPE_OK;
+    return check_device_status(h);
 }
 
 long long gpe_kernel_launches(const gpe_handle* h) { return h ? h->launches : 0; }
+
+gpe_status gpe_profile_enable(gpe_handle* h, int enable) {
+    GPE_TRY(check_handle(h));
+    h->prof = enable != 0;
+    return GPE_OK;
+}
+
+gpe_status gpe_profile_read(gpe_handle* h, double* ms_out, long long* count_out) {
+    GPE_TRY(check_handle(h));
+    GPE_CUDA(cudaStreamSynchronize(h->st));
+    double ms[GPE_PROF_KINDS] = {0};
+    long long cnt[GPE_PROF_KINDS] = {0};
+    for (auto& r : h->recs) {
+        float t = 0.f;
+        GPE_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+        ms[r.kind] += t;
+        cnt[r.kind] += 1;
+        h->ev_free.push_back(r.a);
+        h->ev_free.push_back(r.b);
+    }
+    h->recs.clear();
+    for (int k = 0; k < GPE_PROF_KINDS; ++k) {
+        if (ms_out) ms_out[k] = ms[k];
+        if (count_out) count_out[k] = cnt[k];
+    }
+    return GPE_OK;
+}
 
 }  // extern "C"

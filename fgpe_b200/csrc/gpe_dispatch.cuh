@@ -9,39 +9,30 @@ namespace gpe {
 
 #define GPE_FAMILIES(X) X(p2) X(p3) X(p5) X(p9)
 
-#define GPE_DECL_FAMILY(F)                                                                                       \
-    bool dispatch_x_##F##_f(int L, int NF, const PassArgs<float>& a, cudaStream_t st, cudaError_t* err);        \
-    bool dispatch_s_##F##_f(int L, int NF, const PassArgs<float>& a, int nouter, cudaStream_t st,               \
-                            cudaError_t* err);                                                                   \
-    bool dispatch_x_##F##_d(int L, int NF, const PassArgs<double>& a, cudaStream_t st, cudaError_t* err);       \
-    bool dispatch_s_##F##_d(int L, int NF, const PassArgs<double>& a, int nouter, cudaStream_t st,              \
-                            cudaError_t* err);
+#define GPE_DECL_ONE(F, P, R, NF)                                                                      \
+    bool dispatch_x_##F##_##P##_##NF(int L, const PassArgs<R>& a, int rows, size_t smem, cudaStream_t st, cudaError_t* err);    \
+    bool dispatch_s_##F##_##P##_##NF(int L, const PassArgs<R>& a, int nouter, size_t smem, cudaStream_t st, cudaError_t* err);
+#define GPE_DECL_FAMILY(F) GPE_DECL_ONE(F, f, float, 1) GPE_DECL_ONE(F, f, float, 2) \
+                           GPE_DECL_ONE(F, d, double, 1) GPE_DECL_ONE(F, d, double, 2)
 GPE_FAMILIES(GPE_DECL_FAMILY)
 #undef GPE_DECL_FAMILY
+#undef GPE_DECL_ONE
 
-inline bool dispatch_x(int L, int NF, const PassArgs<float>& a, cudaStream_t st, cudaError_t* err) {
-#define GPE_TRY(F) if (dispatch_x_##F##_f(L, NF, a, st, err)) return true;
-    GPE_FAMILIES(GPE_TRY)
-#undef GPE_TRY
-    return false;
-}
-inline bool dispatch_x(int L, int NF, const PassArgs<double>& a, cudaStream_t st, cudaError_t* err) {
-#define GPE_TRY(F) if (dispatch_x_##F##_d(L, NF, a, st, err)) return true;
-    GPE_FAMILIES(GPE_TRY)
-#undef GPE_TRY
-    return false;
-}
-inline bool dispatch_s(int L, int NF, const PassArgs<float>& a, int nouter, cudaStream_t st, cudaError_t* err) {
-#define GPE_TRY(F) if (dispatch_s_##F##_f(L, NF, a, nouter, st, err)) return true;
-    GPE_FAMILIES(GPE_TRY)
-#undef GPE_TRY
-    return false;
-}
-inline bool dispatch_s(int L, int NF, const PassArgs<double>& a, int nouter, cudaStream_t st, cudaError_t* err) {
-#define GPE_TRY(F) if (dispatch_s_##F##_d(L, NF, a, nouter, st, err)) return true;
-    GPE_FAMILIES(GPE_TRY)
-#undef GPE_TRY
-    return false;
-}
+#define GPE_DISPATCH_FN(R, P)                                                                        \
+    inline bool dispatch_x(int L, int NF, const PassArgs<R>& a, int rows, size_t smem, cudaStream_t st, cudaError_t* err) { \
+        GPE_FAMILIES(GPE_TRYX_##P)                                                                   \
+        return false;                                                                                \
+    }                                                                                                \
+    inline bool dispatch_s(int L, int NF, const PassArgs<R>& a, int nouter, size_t smem, cudaStream_t st, \
+                           cudaError_t* err) {                                                       \
+        GPE_FAMILIES(GPE_TRYS_##P)                                                                   \
+        return false;                                                                                \
+    }
+#define GPE_TRYX_f(F) if (NF == 1 ? dispatch_x_##F##_f_1(L, a, rows, smem, st, err) : dispatch_x_##F##_f_2(L, a, rows, smem, st, err)) return true;
+#define GPE_TRYX_d(F) if (NF == 1 ? dispatch_x_##F##_d_1(L, a, rows, smem, st, err) : dispatch_x_##F##_d_2(L, a, rows, smem, st, err)) return true;
+#define GPE_TRYS_f(F) if (NF == 1 ? dispatch_s_##F##_f_1(L, a, nouter, smem, st, err) : dispatch_s_##F##_f_2(L, a, nouter, smem, st, err)) return true;
+#define GPE_TRYS_d(F) if (NF == 1 ? dispatch_s_##F##_d_1(L, a, nouter, smem, st, err) : dispatch_s_##F##_d_2(L, a, nouter, smem, st, err)) return true;
+GPE_DISPATCH_FN(float, f)
+GPE_DISPATCH_FN(double, d)
 
 }  // namespace gpe

@@ -1,24 +1,24 @@
 // gpe_inst_body.cuh -- included by gpe_inst_*.cu after defining GPE_R (float
-// or double), GPE_SFX (f or d), GPE_FAM (family name) and GPE_SIZES(X).
+// or double), GPE_SFX (f or d), GPE_FAM (length family), GPE_NF (fields per
+// pass, 1 or 2) and GPE_SIZES(X).
 #include "gpe_kernels_impl.cuh"
 
 #define GPE_CAT2(a, b) a##b
 #define GPE_CAT(a, b) GPE_CAT2(a, b)
-#define GPE_CAT4(a, b, c, d) GPE_CAT(GPE_CAT(a, b), GPE_CAT(c, d))
+#define GPE_NAME(kind) GPE_CAT(GPE_CAT(GPE_CAT(kind, GPE_FAM), GPE_CAT(_, GPE_SFX)), GPE_CAT(_, GPE_NF))
 
 namespace gpe {
 
-#define GPE_XCASE(L)                                                                        \
-    case L:                                                                                 \
-        *err = (NF == 1) ? launch_xpass<GPE_R, L, 1>(a, st) : launch_xpass<GPE_R, L, 2>(a, st); \
+#define GPE_XCASE(L)                                     \
+    case L:                                              \
+        *err = launch_xpass<GPE_R, L, GPE_NF>(a, rows, smem, st);    \
         return true;
-#define GPE_SCASE(L)                                                                                          \
-    case L:                                                                                                   \
-        *err = (NF == 1) ? launch_spass<GPE_R, L, 1>(a, nouter, st) : launch_spass<GPE_R, L, 2>(a, nouter, st); \
+#define GPE_SCASE(L)                                             \
+    case L:                                                      \
+        *err = launch_spass<GPE_R, L, GPE_NF>(a, nouter, smem, st);    \
         return true;
 
-bool GPE_CAT4(dispatch_x_, GPE_FAM, _, GPE_SFX)(int L, int NF, const PassArgs<GPE_R>& a, cudaStream_t st,
-                                                cudaError_t* err) {
+bool GPE_NAME(dispatch_x_)(int L, const PassArgs<GPE_R>& a, int rows, size_t smem, cudaStream_t st, cudaError_t* err) {
     switch (L) {
         GPE_SIZES(GPE_XCASE)
         default:
@@ -26,8 +26,7 @@ bool GPE_CAT4(dispatch_x_, GPE_FAM, _, GPE_SFX)(int L, int NF, const PassArgs<GP
     }
 }
 
-bool GPE_CAT4(dispatch_s_, GPE_FAM, _, GPE_SFX)(int L, int NF, const PassArgs<GPE_R>& a, int nouter, cudaStream_t st,
-                                                cudaError_t* err) {
+bool GPE_NAME(dispatch_s_)(int L, const PassArgs<GPE_R>& a, int nouter, size_t smem, cudaStream_t st, cudaError_t* err) {
     switch (L) {
         GPE_SIZES(GPE_SCASE)
         default:

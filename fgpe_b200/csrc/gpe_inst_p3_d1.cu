@@ -1,7 +1,8 @@
-// Pass-kernel instantiations: length family p3, double.
+// Pass-kernel instantiations: length family p3, double, 1 field(s) per pass.
 #include "gpe_sizes.h"
 #define GPE_R double
 #define GPE_SFX d
 #define GPE_FAM p3
+#define GPE_NF 1
 #define GPE_SIZES(X) GPE_SIZES_p3(X)
 #include "gpe_inst_body.cuh"

@@ -1,0 +1,8 @@
+// Pass-kernel instantiations: length family p5, double, 2 field(s) per pass.
+#include "gpe_sizes.h"
+#define GPE_R double
+#define GPE_SFX d
+#define GPE_FAM p5
+#define GPE_NF 2
+#define GPE_SIZES(X) GPE_SIZES_p5(X)
+#include "gpe_inst_body.cuh"

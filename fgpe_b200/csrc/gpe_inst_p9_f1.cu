@@ -1,0 +1,8 @@
+// Pass-kernel instantiations: length family p9, float, 1 field(s) per pass.
+#include "gpe_sizes.h"
+#define GPE_R float
+#define GPE_SFX f
+#define GPE_FAM p9
+#define GPE_NF 1
+#define GPE_SIZES(X) GPE_SIZES_p9(X)
+#include "gpe_inst_body.cuh"

@@ -20,6 +20,7 @@
 
 #include "gpe_common.cuh"
 #include "gpe_fft.cuh"
+#include "gpe_tma.cuh"
 #include "../../include/gpe.h"
 
 namespace gpe {
@@ -39,9 +40,20 @@ enum EpiOp {
     EPI_OBS = 4,     // reductions of |psi|^2, Re(psi* h_mu), Re(psi* h_en)
     EPI_RKI = 5      // imaginary-time RK4 stage
 };
-enum SpecOp { SPEC_NONE = 0, SPEC_KIN = 1 };
+enum SpecOp { SPEC_NONE = 0, SPEC_KIN = 1, SPEC_PX = 2 };
+// Compile-time role of an x-pass kernel: forward only, inverse + one epilogue
+// family, or the x-only full pass (run-time epilogue).  Specialising keeps the
+// register count and code size of each kernel to what its role needs.
+// XK_RK runs the real-time stages without reductions (the hot path); XK_RKO
+// is the same stage with the logging reductions of the last step of a chunk.
+enum XKind { XK_FWD = 0, XK_STORE = 1, XK_RK = 2, XK_HB = 3, XK_RKI = 4, XK_AH = 5, XK_FULL = 6, XK_RKO = 7 };
+constexpr int NXKIND = 8;  // SPEC_PX: BECVPx, src/parallel.cu:283-292
 
-constexpr int MAXQ = 6;  // reduced quantities per launch (3 per component)
+constexpr int MAXQ = 6;       // reduced quantities per launch (3 per component)
+constexpr int MAXSTAGE = 12;  // input fields staged in shared memory per launch
+// Source of a staged field: a fixed pointer, or the current / previous
+// heavy-ball buffer of a component (chosen on the device from cur_slot).
+enum StageKind { SK_FIXED = 0, SK_CUR = 1, SK_OLD = 2 };
 
 template <typename R>
 struct PassArgs {
@@ -74,12 +86,24 @@ struct PassArgs {
     double dt, beta, lap_scale, DV, eps;
     double npart[2];
     double c_re, c_im;       // RK stage coefficient (stage 1..3 axpy; final uses c/6)
+    // Inputs staged in shared memory (slot s holds field stage_*[s] for the
+    // CTA's rows / lines); -1 = not staged.
+    int nstage;
+    int tma;                 // 1: bulk async copies (all alignments hold), 0: plain loads
+    const C* stage_ptr[MAXSTAGE];
+    int stage_kind[MAXSTAGE];
+    int stage_comp[MAXSTAGE];
+    int s_w[3], s_psi[2], s_v[2], s_a[2], s_k[2], s_xo[2];
 };
 
 // ---- shared-memory line addressing -----------------------------------------
-template <typename C> struct RowAddr {      // X pass: S[b*L + pos]
+// X pass exchange rows are padded by one slot every 8 elements: the first
+// radix-8 Stockham pass stores with stride 8, which would put the 16 lanes of
+// a row on two bank pairs without the padding.
+__host__ __device__ constexpr int xpad(int L) { return L + (L >> 3); }
+template <typename C> struct RowAddr {      // X pass: S[b*xpad(L) + pos + pos/8]
     C* base;
-    __device__ __forceinline__ C* operator()(int pos) const { return base + pos; }
+    __device__ __forceinline__ C* operator()(int pos) const { return base + pos + (pos >> 3); }
 };
 template <typename C> struct ColAddr {      // strided pass: S[pos*tx + b]
     C* base;
@@ -260,17 +284,11 @@ template <typename R>
 __device__ void finalize_scalars(const PassArgs<R>& a, const double* S);
 
 // ---- kernels ----------------------------------------------------------------
-template <typename R, int L>
-struct XCfg {
-    static constexpr int T = Plan<L>::T;
-    static constexpr int B = (256 / T) > 0 ? (256 / T) : 1;  // rows per CTA
-    static constexpr int THREADS = B * T;
-};
+
+template <typename R, int L, int NF, int KIND>
+__global__ void __launch_bounds__(256, 1) k_xpass(PassArgs<R> a, int rows, int ntiles);
 
 template <typename R, int L, int NF>
-__global__ void __launch_bounds__(256) k_xpass(PassArgs<R> a);
-
-template <typename R, int L, int NF>
-__global__ void __launch_bounds__(512) k_spass(PassArgs<R> a);
+__global__ void __launch_bounds__(512, 1) k_spass(PassArgs<R> a, int ntx, int ntiles);
 
 }  // namespace gpe

@@ -1,6 +1,15 @@
 // gpe_sizes.h -- grid lengths with compiled pass kernels, per family.
+// GPE_DEV_SIZES (make GPE_DEV=1) keeps only the lengths the test suite uses,
+// for quick kernel rebuilds during development.
 #pragma once
+#ifdef GPE_DEV_SIZES
+#define GPE_SIZES_p2(X) X(1) X(4) X(8) X(16) X(32) X(64) X(128)
+#define GPE_SIZES_p3(X) X(6) X(12) X(24) X(96)
+#define GPE_SIZES_p5(X) X(5) X(10) X(20) X(25)
+#define GPE_SIZES_p9(X) X(9)
+#else
 #define GPE_SIZES_p2(X) X(1) X(2) X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
 #define GPE_SIZES_p3(X) X(3) X(6) X(12) X(24) X(48) X(96) X(192) X(384) X(768)
 #define GPE_SIZES_p5(X) X(5) X(10) X(20) X(40) X(80) X(160) X(320) X(640) X(25) X(50) X(100) X(200) X(400) X(800)
 #define GPE_SIZES_p9(X) X(9) X(18) X(36) X(72) X(144) X(288) X(576) X(27) X(54) X(108) X(216) X(432) X(864)
+#endif

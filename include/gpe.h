@@ -177,6 +177,10 @@ gpe_status gpe_apply_h(gpe_handle* h, double t, int comp,
  * alg_calc2Observables (src/baseHamiltonian.cu:173-179,230-236) divide these
  * by the caller's norm. */
 gpe_status gpe_observables(gpe_handle* h, double t, double* out);
+/* BaseHamiltonian::alg_calcPx (src/baseHamiltonian.cu:184-195) before the
+ * plugin's division: sum Re(conj(psi) IFFT(kx FFT psi)) DV with the
+ * unnormalised inverse transform of the reference (kx in cycles/length). */
+gpe_status gpe_momentum_x(gpe_handle* h, int comp, double* px);
 /* Unnormalised 3D DFT of psi_comp in place, sign -1 (CUFFT_FORWARD) or +1
  * (CUFFT_INVERSE): the cufftExecZ2Z calls of src/baseHamiltonian.cu:89,95. */
 gpe_status gpe_fft(gpe_handle* h, int comp, int sign);
@@ -185,6 +189,19 @@ gpe_status gpe_fft(gpe_handle* h, int comp, int sign);
 gpe_status gpe_sync(gpe_handle* h);
 /* Number of this library's kernels launched by the handle so far. */
 long long  gpe_kernel_launches(const gpe_handle* h);
+
+/* ---- measurement (no counterpart in the reference, whose only timing is
+ * unsynchronised host chrono, src/oneComponentGPSolver.cu:153,197-200) ----- */
+#define GPE_PROF_KINDS 6
+/* Pass kinds: 0 x-forward (+prologue), 1 x-inverse (+epilogue), 2 x-full,
+ * 3 strided forward, 4 strided inverse, 5 strided forward*k-space*inverse. */
+/* When enabled, every pass launch is bracketed by CUDA events on the
+ * handle's stream. */
+gpe_status gpe_profile_enable(gpe_handle* h, int enable);
+/* Synchronises the stream and returns, per pass kind, the summed event time
+ * in ms and the launch count since the previous read (arrays of
+ * GPE_PROF_KINDS; either may be NULL). */
+gpe_status gpe_profile_read(gpe_handle* h, double* ms_out, long long* count_out);
 
 #ifdef __cplusplus
 }

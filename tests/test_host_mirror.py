@@ -1,0 +1,121 @@
+"""Host mirror (fgpe_b200/host, via include/gpe_host.h) against the reference's
+own host classes compiled from its sources (oracle/_ref/libref_host.so, see
+oracle/ref.mk): input parsing, unit conversion, initial psi (including the
+seeded noise), Vext and info.wtxt must be bit-identical.  Runs on CPU."""
+import ctypes
+import os
+import shutil
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libref_host.so")
+INPUTS = os.path.join(ROOT, "tests", "inputs")
+CASES = ["bec_harmonic_3d.txt", "bec_tube_3d.txt", "bec_2d.txt", "bec2_3d.txt", "bec2_tube.txt"]
+
+needs_ref = pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference host library not built (oracle/ref.mk)")
+
+
+def ours():
+    import fgpe_b200 as gp
+    L = gp.lib()
+    P = ctypes.POINTER(ctypes.c_double)
+    L.gpeh_params.argtypes = [ctypes.c_char_p, P]
+    L.gpeh_init_psi.argtypes = [ctypes.c_char_p, ctypes.c_int, P]
+    L.gpeh_init_vext.argtypes = [ctypes.c_char_p, ctypes.c_int, P]
+    L.gpeh_write_info.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, P, ctypes.c_void_p]
+    L.gpeh_last_error.restype = ctypes.c_char_p
+    return L
+
+
+def ref():
+    L = ctypes.CDLL(REF_LIB)
+    P = ctypes.POINTER(ctypes.c_double)
+    L.ref_params.argtypes = [ctypes.c_char_p, P]
+    L.ref_init_psi.argtypes = [ctypes.c_char_p, ctypes.c_int, P]
+    L.ref_init_vext.argtypes = [ctypes.c_char_p, ctypes.c_int, P]
+    L.ref_write_info.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, P, ctypes.c_void_p]
+    return L
+
+
+def materialise(case, tmp_path):
+    src = open(os.path.join(INPUTS, case)).read().replace("@OUT@", str(tmp_path) + "/run_")
+    fn = tmp_path / case
+    fn.write_text(src)
+    return str(fn).encode()
+
+
+def dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+@needs_ref
+@pytest.mark.parametrize("case", CASES)
+def test_params_bit_identical(case, tmp_path):
+    f = materialise(case, tmp_path)
+    a = np.zeros(47)
+    b = np.zeros(47)
+    na = ours().gpeh_params(f, dp(a))
+    nb = ref().ref_params(f, dp(b))
+    assert na == nb
+    assert np.array_equal(a, b), np.nonzero(a != b)
+
+
+@needs_ref
+@pytest.mark.parametrize("case", CASES)
+def test_initial_psi_and_vext_bit_identical(case, tmp_path):
+    f = materialise(case, tmp_path)
+    p = np.zeros(47)
+    nc = ours().gpeh_params(f, dp(p))
+    n = int(p[4])
+    types = [0] if nc == 1 else [1, 2]
+    for t in types:
+        for fn_o, fn_r in (("gpeh_init_psi", "ref_init_psi"), ("gpeh_init_vext", "ref_init_vext")):
+            a = np.zeros(n, np.complex128)
+            b = np.zeros(n, np.complex128)
+            assert getattr(ours(), fn_o)(f, t, dp(a.view(np.float64))) == 0
+            getattr(ref(), fn_r)(f, t, dp(b.view(np.float64)))
+            assert np.array_equal(a.view(np.float64), b.view(np.float64)), (fn_o, t)
+
+
+@needs_ref
+@pytest.mark.parametrize("case", CASES)
+def test_info_wtxt_identical(case, tmp_path):
+    f = materialise(case, tmp_path)
+    names = (ctypes.c_char_p * 3)(b"en", b"mu", b"convergence")
+    units = (ctypes.c_char_p * 3)(b"code", b"code", b"code")
+    vals = np.array([1.2345678901, -0.5, 3e-9])
+    ref().ref_write_info(f, 7, 3, names, dp(vals), units)
+    info = tmp_path / "run_info.wtxt"
+    want = info.read_bytes()
+    info.unlink()
+    assert ours().gpeh_write_info(f, 7, 3, names, dp(vals), units) == 0
+    assert info.read_bytes() == want
+
+
+def test_missing_key_is_an_error_not_exit(tmp_path):
+    src = open(os.path.join(INPUTS, "bec_2d.txt")).read().replace("@OUT@", str(tmp_path) + "/run_")
+    src = "\n".join(l for l in src.splitlines() if not l.startswith("mass"))
+    fn = tmp_path / "bad.txt"
+    fn.write_text(src)
+    out = np.zeros(47)
+    assert ours().gpeh_params(str(fn).encode(), dp(out)) == -1
+    assert b"mass" in ours().gpeh_last_error()
+
+
+def test_missing_file_is_an_error(tmp_path):
+    out = np.zeros(47)
+    assert ours().gpeh_params(str(tmp_path / "nope.txt").encode(), dp(out)) == -1
+
+
+def test_input_typing_rules(tmp_path):
+    # "1E-7" parses as int 1 and double 1e-7 (stoi/stod prefixes,
+    # src/input_variables.cu:55-74); later duplicates override earlier lines.
+    src = open(os.path.join(INPUTS, "bec_2d.txt")).read().replace("@OUT@", str(tmp_path) + "/run_")
+    src += "\nniter 1E-7 # int prefix\nnx 32\n"
+    fn = tmp_path / "t.txt"
+    fn.write_text(src)
+    out = np.zeros(47)
+    assert ours().gpeh_params(str(fn).encode(), dp(out)) == 1
+    assert out[22] == 1 and out[0] == 32
