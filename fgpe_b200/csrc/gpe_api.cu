@@ -50,6 +50,12 @@ enum StateMode { ST_CANON = 0, ST_HB = 1, ST_RKI = 2 };
 
 }  // namespace
 
+// Lets other translation units of the library (gpe_noalloc.cu) record the
+// message that gpe_last_error_string() returns.
+namespace gpe {
+void set_last_error(const char* msg) { g_err = msg; }
+}  // namespace gpe
+
 struct gpe_handle {
     gpe_config cfg;
     int prec = GPE_C128;

@@ -185,6 +185,23 @@ gpe_status gpe_momentum_x(gpe_handle* h, int comp, double* px);
  * (CUFFT_INVERSE): the cufftExecZ2Z calls of src/baseHamiltonian.cu:89,95. */
 gpe_status gpe_fft(gpe_handle* h, int comp, int sign);
 
+/* ---- allocation-free norm (no counterpart in the reference) -------------
+ * dev_out[0] = DV * sum |psi[i]|^2 over n complex128 points of a caller-owned
+ * device array (interleaved re, im; 16-byte aligned), issued on cuda_stream
+ * (NULL = legacy default stream) and not synchronised.  It needs no handle and
+ * allocates nothing: its block partials live in a fixed 128 KiB device array
+ * inside the library, for callers whose device memory is already reserved by
+ * their own allocator or that must avoid the synchronisation cudaFree
+ * implies.  n above GPE_NORM_NOALLOC_MAX_POINTS is rejected with
+ * GPE_ERR_UNSUPPORTED.  The first call on each device does a one-time set-up
+ * (scratch address lookup, a synchronous zeroing of its completion counter):
+ * make it before any stream capture starts on that device.  Calls that may
+ * overlap on one device share the scratch and race; order them on one stream.
+ * The result is the same bits on every call for the same input. */
+#define GPE_NORM_NOALLOC_MAX_POINTS 134217728LL /* 512^3 */
+gpe_status gpe_norm_noalloc(const void* dev_psi_c128, long long n, double dv, double* dev_out,
+                            void* cuda_stream);
+
 /* Synchronise the handle's stream and report any asynchronous error. */
 gpe_status gpe_sync(gpe_handle* h);
 /* Number of this library's kernels launched by the handle so far. */
