@@ -80,6 +80,9 @@ struct gpe_handle {
     long long launches = 0;
     int mode = ST_CANON;
     bool hb_old_valid = true;
+    // W[0..nf-1] hold the x-forward transform of the state in A (left by the
+    // last real-time stage); any other operation clears it.
+    bool w_fwd_A = false;
     // per-pass event timing (gpe_profile_enable)
     bool prof = false;
     std::vector<cudaEvent_t> ev_free;
@@ -285,126 +288,42 @@ int prof_kind(int mode) {
     }
 }
 
-// Shared-memory budget of one pass CTA (staged slots + FFT exchange buffer).
-constexpr size_t SMEM_BUDGET = 96 * 1024;
-
-template <typename R>
-struct Stager {
-    typedef typename Cx<R>::T C;
-    PassArgs<R>& a;
-    explicit Stager(PassArgs<R>& a_) : a(a_) {
-        a.nstage = 0;
-        for (int i = 0; i < 3; ++i) a.s_w[i] = -1;
-        for (int i = 0; i < 2; ++i) a.s_psi[i] = a.s_v[i] = a.s_a[i] = a.s_k[i] = a.s_xo[i] = -1;
-    }
-    int add(const C* p, int kind, int comp) {
-        const int s = a.nstage++;
-        a.stage_ptr[s] = p;
-        a.stage_kind[s] = kind;
-        a.stage_comp[s] = comp;
-        return s;
-    }
-    // psi source of the prologue / epilogue per a.pro
-    void psi(int npsi) {
-        for (int c = 0; c < npsi; ++c) {
-            if (a.s_psi[c] >= 0) continue;
-            if (a.pro == PRO_PIN) a.s_psi[c] = add(a.pin[c], SK_FIXED, c);
-            else if (a.pro == PRO_CUR) a.s_psi[c] = add(nullptr, SK_CUR, c);
-            else a.s_psi[c] = add(a.buf[0][c], SK_FIXED, c);
-        }
-    }
-    // Fields read by the epilogue op (see epilogue_point).
-    void epilogue(int npsi) {
-        switch (a.epi) {
-            case EPI_STORE:
-                return;
-            case EPI_RK:
-                psi(npsi);
-                for (int c = 0; c < npsi; ++c) {
-                    a.s_v[c] = add(a.vext[c], SK_FIXED, c);
-                    if (a.stage > 1) {
-                        a.s_a[c] = add(a.buf[0][c], SK_FIXED, c);
-                        a.s_k[c] = add(a.kacc[c], SK_FIXED, c);
-                    }
-                }
-                return;
-            case EPI_HB:
-                psi(npsi);
-                for (int c = 0; c < npsi; ++c) {
-                    a.s_xo[c] = add(nullptr, SK_OLD, c);
-                    a.s_v[c] = add(a.vext[c], SK_FIXED, c);
-                }
-                return;
-            case EPI_RKI:
-                for (int c = 0; c < npsi; ++c) {
-                    if (a.stage == 1 && a.pro == PRO_A_SCALED) {
-                        psi(npsi);
-                        a.s_a[c] = a.s_psi[c];
-                    } else {
-                        a.s_a[c] = add(a.buf[0][c], SK_FIXED, c);
-                        if (a.stage > 1) {
-                            if (a.s_psi[c] < 0) a.s_psi[c] = add(a.pin[c], SK_FIXED, c);
-                            a.s_k[c] = add(a.kacc[c], SK_FIXED, c);
-                        }
-                    }
-                    a.s_v[c] = add(a.vext[c], SK_FIXED, c);
-                }
-                return;
-            default:  // EPI_APPLYH, EPI_OBS
-                psi(npsi);
-                for (int c = 0; c < npsi; ++c) a.s_v[c] = add(a.vext[c], SK_FIXED, c);
-                return;
-        }
-    }
-};
-
+// x pass: `rows` lines of T threads per CTA (256 threads when the line allows),
+// one padded shared-memory exchange row per line.
 template <typename R>
 gpe_status launch_x(gpe_handle* h, PassArgs<R> a, int nf, int mode) {
     typedef typename Cx<R>::T C;
     ProfScope ps(h, prof_kind(mode));
     a.mode = mode;
     a.tw = (const C*)h->tw[0];
-    const int npsi = nf - a.dens;
-    Stager<R> sg(a);
-    if (mode == XM_FWD || mode == XM_FULL) sg.psi(npsi);
-    if (mode == XM_INV)
-        for (int f = 0; f < nf; ++f) a.s_w[f] = sg.add(a.w[f], SK_FIXED, f);
-    if (mode == XM_INV || mode == XM_FULL) sg.epilogue(npsi);
     const int L = h->nx;
-    // 2 staging buffers + padded exchange buffers (one per field: the
-    // inverse results of all fields meet in the epilogue)
-    const size_t row_bytes = ((size_t)2 * a.nstage * L + (size_t)nf * xpad(L)) * sizeof(C);
     const int T = plan_T(L);
-    const int bmax = (256 / T) > 0 ? 256 / T : 1;
-    int rows = (int)(SMEM_BUDGET / row_bytes);
-    if (rows > bmax) rows = bmax;
-    if (rows < 1) rows = 1;
-    if ((size_t)rows * row_bytes > 220 * 1024)
-        return fail(GPE_ERR_UNSUPPORTED, "x-pass tile does not fit in shared memory (length " + std::to_string(L) + ")");
-    a.tma = ((size_t)L * sizeof(C)) % 16 == 0 ? 1 : 0;
+    const int rows = (256 / T) > 0 ? 256 / T : 1;
+    const size_t smem = (size_t)rows * xpad(L) * sizeof(C);
     cudaError_t err = cudaSuccess;
-    if (!dispatch_x(L, nf, a, rows, (size_t)rows * row_bytes, h->st, &err))
+    if (!dispatch_x(L, nf, a, rows, smem, h->st, &err))
         return fail(GPE_ERR_UNSUPPORTED, "no x-pass kernel for length " + std::to_string(L));
     if (err != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("x pass launch: ") + cudaGetErrorString(err));
     h->launches++;
     return GPE_OK;
 }
 
+// Strided pass along y (axis 1) or z (axis 2): tx consecutive x values per
+// CTA, 128-byte rows (16 complex64 / 8 complex128 values) when nx allows,
+// at most 256 threads.
 template <typename R>
 gpe_status launch_s(gpe_handle* h, PassArgs<R> a, int nf, int axis, int mode) {
     typedef typename Cx<R>::T C;
     ProfScope ps(h, prof_kind(mode));
     const int L = axis == 1 ? h->ny : h->nz;
     const int T = plan_T(L);
-    int tx = h->nx < 16 ? h->nx : 16;
-    while (tx > 1 && tx * T > 512) tx /= 2;
-    while (tx > 1 && (size_t)(2 * nf + 1) * L * tx * sizeof(C) > SMEM_BUDGET) tx /= 2;
+    int tx = (int)(128 / sizeof(C));
+    if (tx > h->nx) tx = h->nx;
+    while (tx > 1 && tx * T > 256) tx /= 2;
     a.mode = mode;
     a.sax = axis;
     a.tx = tx;
     a.tw = (const C*)h->tw[axis];
-    Stager<R> sg(a);
-    for (int f = 0; f < nf; ++f) a.s_w[f] = sg.add(a.w[f], SK_FIXED, f);
     int nouter;
     if (axis == 1) {
         a.sstride = h->nx;
@@ -415,9 +334,7 @@ gpe_status launch_s(gpe_handle* h, PassArgs<R> a, int nf, int axis, int mode) {
         a.ostride = h->nx;
         nouter = h->ny;
     }
-    const size_t es = sizeof(C);
-    a.tma = ((h->nx * es) % 16 == 0 && (tx * es) % 16 == 0 && ((h->nx % tx) * es) % 16 == 0) ? 1 : 0;
-    const size_t smem = (size_t)(2 * nf + 1) * L * tx * es;
+    const size_t smem = (size_t)L * tx * sizeof(C);
     cudaError_t err = cudaSuccess;
     if (!dispatch_s(L, nf, a, nouter, smem, h->st, &err))
         return fail(GPE_ERR_UNSUPPORTED, "no strided-pass kernel for length " + std::to_string(L));
@@ -429,13 +346,14 @@ gpe_status launch_s(gpe_handle* h, PassArgs<R> a, int nf, int axis, int mode) {
 // Full kinetic chain: x-forward with prologue, strided forward passes, the
 // last strided axis forward * k-space * inverse, strided inverse passes,
 // x-inverse with epilogue.  a.pro / a.epi / a.stage ... are set by the caller.
+// skip_fwd: W already holds the x-forward transform of the stage input.
 template <typename R>
-gpe_status run_chain(gpe_handle* h, const PassArgs<R>& a, int nf) {
+gpe_status run_chain(gpe_handle* h, const PassArgs<R>& a, int nf, bool skip_fwd = false) {
     int axes[2], na = 0;
     if (h->ny > 1) axes[na++] = 1;
     if (h->nz > 1) axes[na++] = 2;
     if (na == 0) return launch_x<R>(h, a, nf, XM_FULL);
-    GPE_TRY(launch_x<R>(h, a, nf, XM_FWD));
+    if (!skip_fwd) GPE_TRY(launch_x<R>(h, a, nf, XM_FWD));
     for (int i = 0; i < na - 1; ++i) GPE_TRY(launch_s<R>(h, a, nf, axes[i], SM_FWD));
     GPE_TRY(launch_s<R>(h, a, nf, axes[na - 1], SM_FKI));
     for (int i = na - 2; i >= 0; --i) GPE_TRY(launch_s<R>(h, a, nf, axes[i], SM_INV));
@@ -462,6 +380,7 @@ template <typename R>
 gpe_status canonicalize_t(gpe_handle* h) {
     typedef typename Cx<R>::T C;
     if (h->mode == ST_CANON) return GPE_OK;
+    h->w_fwd_A = false;
     const int thr = 256;
     for (int c = 0; c < h->ncomp; ++c) {
         k_canon<C><<<blocks_for(h->N, thr), thr, 0, h->st>>>((C*)h->A[c], (C*)h->B[c], h->sc, c, h->mode == ST_HB,
@@ -498,6 +417,12 @@ gpe_status step_real_t(gpe_handle* h, int first, int nsteps, double* obs_out) {
     PassArgs<R> a = base_args<R>(h);
     a.epi = EPI_RK;
     a.pro = PRO_PIN;
+    // Each stage's x-inverse epilogue also x-forward transforms the state it
+    // writes (the next stage's input) unless it runs the logging reductions;
+    // the next stage then starts at the strided passes.
+    const bool can_fuse = h->ny > 1 || h->nz > 1;
+    bool w_ready = can_fuse && h->w_fwd_A;
+    h->w_fwd_A = false;
     for (int j = 0; j < nsteps; ++j) {
         const int it = first + j;
         for (int s = 1; s <= 4; ++s) {
@@ -508,9 +433,12 @@ gpe_status step_real_t(gpe_handle* h, int first, int nsteps, double* obs_out) {
             a.c_im = (s <= 2) ? -0.5 * dt : -1.0 * dt;
             a.t = (s == 1) ? (double)it * dt : (s < 4) ? (it + 0.5) * dt : (double)(it + 1) * dt;
             a.want_obs = (obs_out != nullptr && j == nsteps - 1 && s == 4) ? 1 : 0;
-            GPE_TRY(run_chain<R>(h, a, h->nf));
+            a.fuse_fwd = (can_fuse && !a.want_obs) ? 1 : 0;
+            GPE_TRY(run_chain<R>(h, a, h->nf, w_ready));
+            w_ready = a.fuse_fwd != 0;
         }
     }
+    h->w_fwd_A = w_ready;
     if (obs_out && nsteps > 0) {
         DevScalars s;
         GPE_TRY(sync_read_scalars(h, &s));
@@ -523,6 +451,7 @@ gpe_status step_real_t(gpe_handle* h, int first, int nsteps, double* obs_out) {
 
 template <typename R>
 gpe_status step_imag_t(gpe_handle* h, int first, int nsteps, int* iters_done, int* converged) {
+    h->w_fwd_A = false;
     typedef typename Cx<R>::T C;
     const double dt = h->cfg.dt;
     const bool rk = h->cfg.imag_scheme == GPE_IMAG_RK4;
@@ -574,6 +503,7 @@ gpe_status step_imag_t(gpe_handle* h, int first, int nsteps, int* iters_done, in
 
 template <typename R>
 gpe_status apply_chain_t(gpe_handle* h, int epi, double t, int comp_only, int spec = SPEC_KIN) {
+    h->w_fwd_A = false;
     GPE_TRY(canonicalize_t<R>(h));
     PassArgs<R> a = base_args<R>(h);
     a.pro = PRO_PIN;
@@ -594,6 +524,7 @@ gpe_status apply_chain_t(gpe_handle* h, int epi, double t, int comp_only, int sp
 
 template <typename R>
 gpe_status fft_t(gpe_handle* h, int comp, int sign) {
+    h->w_fwd_A = false;
     typedef typename Cx<R>::T C;
     GPE_TRY(canonicalize_t<R>(h));
     PassArgs<R> a = base_args<R>(h);
@@ -871,6 +802,7 @@ gpe_status gpe_set_params(gpe_handle* h, const double prms[GPE_NO_HAMIL_PARAMS])
 }
 
 gpe_status gpe_set_psi(gpe_handle* h, int comp, const double* host_c128) {
+    if (h) h->w_fwd_A = false;
     GPE_TRY(check_handle(h));
     GPE_TRY(check_comp(h, comp));
     if (!host_c128) return fail(GPE_ERR_INVALID_ARG, "null psi");
@@ -883,6 +815,7 @@ gpe_status gpe_set_psi(gpe_handle* h, int comp, const double* host_c128) {
 }
 
 gpe_status gpe_set_psi_device(gpe_handle* h, int comp, const void* dev_c128) {
+    if (h) h->w_fwd_A = false;
     GPE_TRY(check_handle(h));
     GPE_TRY(check_comp(h, comp));
     if (!dev_c128) return fail(GPE_ERR_INVALID_ARG, "null psi");

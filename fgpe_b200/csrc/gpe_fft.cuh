@@ -77,10 +77,14 @@ struct Plan {
     __host__ __device__ static constexpr int out_radix(bool rev) { return M == 0 ? 1 : radix(M - 1, rev); }
 };
 
-// Line position of register e for a pattern of radix Rr.
+// Line position of register e for a pattern of radix Rr: t + reg_off(e).
+template <int L, int E, int T, int Rr>
+__host__ __device__ constexpr int reg_off(int e) {
+    return (e / Rr) * T + (e % Rr) * (L / Rr);
+}
 template <int L, int E, int T, int Rr>
 __device__ __forceinline__ int reg_pos(int t, int e) {
-    return t + (e / Rr) * T + (e % Rr) * (L / Rr);
+    return t + reg_off<L, E, T, Rr>(e);
 }
 
 // ---- small DFTs, X_q = sum_r x_r exp(SIGN 2 pi i r q / R) ------------------
@@ -173,8 +177,11 @@ template <int SIGN, typename C> struct Butterfly<5, SIGN, C> {
 // ---- Stockham passes ---------------------------------------------------------
 // Addr: functor, C* operator()(int pos) -> shared-memory slot of line position pos.
 // tw: forward roots of unity exp(-2 pi i m/L), m in [0, L).
+// Index arithmetic is unsigned so that (t + q*T) / Ns and % Ns split into a
+// per-thread part and a compile-time part whenever T is a multiple of Ns.
 template <int L, int P, int SIGN, bool REV, typename C, typename Addr>
-__device__ __forceinline__ void fft_passes(C (&v)[Plan<L>::E], const Addr& addr, const C* __restrict__ tw, int t) {
+__device__ __forceinline__ void fft_passes(C (&v)[Plan<L>::E], const Addr& addr, const C* __restrict__ tw,
+                                           unsigned t) {
     constexpr int M = Plan<L>::M;
     if constexpr (P < M) {
         constexpr int R = Plan<L>::radix(P, REV);
@@ -186,16 +193,16 @@ __device__ __forceinline__ void fft_passes(C (&v)[Plan<L>::E], const Addr& addr,
 #pragma unroll
             for (int q = 0; q < G; ++q)
 #pragma unroll
-                for (int r = 0; r < R; ++r) v[q * R + r] = *addr(t + q * T + r * (L / R));
+                for (int r = 0; r < R; ++r) v[q * R + r] = *addr(t + (unsigned)(q * T + r * (L / R)));
         }
 #pragma unroll
         for (int q = 0; q < G; ++q) {
             if constexpr (Ns > 1) {
-                const int j = t + q * T;
-                const int k = j % Ns;
+                const unsigned j = t + (unsigned)(q * T);
+                const unsigned k = j % (unsigned)Ns;
 #pragma unroll
                 for (int r = 1; r < R; ++r) {
-                    const C w = tw[r * k * (L / (Ns * R))];
+                    const C w = __ldg(tw + (unsigned)r * k * (unsigned)(L / (Ns * R)));
                     v[q * R + r] = (SIGN < 0) ? cmul(v[q * R + r], w) : cmulc(v[q * R + r], w);
                 }
             }
@@ -205,11 +212,11 @@ __device__ __forceinline__ void fft_passes(C (&v)[Plan<L>::E], const Addr& addr,
             __syncthreads();
 #pragma unroll
             for (int q = 0; q < G; ++q) {
-                const int j = t + q * T;
-                const int k = j % Ns;
-                const int idxD = (j / Ns) * Ns * R + k;
+                const unsigned j = t + (unsigned)(q * T);
+                const unsigned k = j % (unsigned)Ns;
+                const unsigned idxD = (j / (unsigned)Ns) * (unsigned)(Ns * R) + k;
 #pragma unroll
-                for (int r = 0; r < R; ++r) *addr(idxD + r * Ns) = v[q * R + r];
+                for (int r = 0; r < R; ++r) *addr(idxD + (unsigned)(r * Ns)) = v[q * R + r];
             }
             __syncthreads();
             fft_passes<L, P + 1, SIGN, REV>(v, addr, tw, t);
@@ -219,13 +226,15 @@ __device__ __forceinline__ void fft_passes(C (&v)[Plan<L>::E], const Addr& addr,
 
 // Forward transform: registers in in_radix(false) pattern -> out_radix(false) pattern.
 template <int L, typename C, typename Addr>
-__device__ __forceinline__ void line_fft_fwd(C (&v)[Plan<L>::E], const Addr& addr, const C* __restrict__ tw, int t) {
+__device__ __forceinline__ void line_fft_fwd(C (&v)[Plan<L>::E], const Addr& addr, const C* __restrict__ tw,
+                                             unsigned t) {
     fft_passes<L, 0, -1, false>(v, addr, tw, t);
 }
 // Inverse (unnormalised) transform with the radices reversed:
 // registers in in_radix(true) == out_radix(false) pattern -> out_radix(true) == in_radix(false).
 template <int L, typename C, typename Addr>
-__device__ __forceinline__ void line_fft_inv(C (&v)[Plan<L>::E], const Addr& addr, const C* __restrict__ tw, int t) {
+__device__ __forceinline__ void line_fft_inv(C (&v)[Plan<L>::E], const Addr& addr, const C* __restrict__ tw,
+                                             unsigned t) {
     fft_passes<L, 0, +1, true>(v, addr, tw, t);
 }
 

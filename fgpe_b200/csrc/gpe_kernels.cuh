@@ -20,7 +20,6 @@
 
 #include "gpe_common.cuh"
 #include "gpe_fft.cuh"
-#include "gpe_tma.cuh"
 #include "../../include/gpe.h"
 
 namespace gpe {
@@ -45,16 +44,14 @@ enum SpecOp { SPEC_NONE = 0, SPEC_KIN = 1, SPEC_PX = 2 };
 // family, or the x-only full pass (run-time epilogue).  Specialising keeps the
 // register count and code size of each kernel to what its role needs.
 // XK_RK runs the real-time stages without reductions (the hot path); XK_RKO
-// is the same stage with the logging reductions of the last step of a chunk.
-enum XKind { XK_FWD = 0, XK_STORE = 1, XK_RK = 2, XK_HB = 3, XK_RKI = 4, XK_AH = 5, XK_FULL = 6, XK_RKO = 7 };
-constexpr int NXKIND = 8;  // SPEC_PX: BECVPx, src/parallel.cu:283-292
+// is the same stage with the logging reductions of the last step of a chunk;
+// XK_RKF is XK_RK followed by the forward x transform of the state it just
+// wrote, which is the x-forward pass of the next stage.
+enum XKind { XK_FWD = 0, XK_STORE = 1, XK_RK = 2, XK_HB = 3, XK_RKI = 4, XK_AH = 5, XK_FULL = 6, XK_RKO = 7,
+             XK_RKF = 8 };
+constexpr int NXKIND = 9;  // SPEC_PX: BECVPx, src/parallel.cu:283-292
 
 constexpr int MAXQ = 6;       // reduced quantities per launch (3 per component)
-constexpr int MAXSTAGE = 12;  // input fields staged in shared memory per launch
-// Source of a staged field: a fixed pointer, or the current / previous
-// heavy-ball buffer of a component (chosen on the device from cur_slot).
-enum StageKind { SK_FIXED = 0, SK_CUR = 1, SK_OLD = 2 };
-
 template <typename R>
 struct PassArgs {
     typedef typename Cx<R>::T C;
@@ -66,6 +63,7 @@ struct PassArgs {
     int mode, pro, epi, spec, stage, ham, sax;
     int check_done;          // exit when sc->done is set (stepping chunks)
     int want_obs;            // RK stage 4: logging reductions
+    int fuse_fwd;            // RK epilogue: also x-forward transform the new state into w
     C* w[3];                 // transformed fields (work buffers)
     C* buf[2][2];            // [slot][comp] state buffers (A = slot 0, B = slot 1)
     C* kacc[2];              // RK accumulators
@@ -79,21 +77,13 @@ struct PassArgs {
     const R* vdd;            // dipolar kernel / N (spectral order) or null
     const double* prms;      // d_h_params
     DevScalars* sc;
-    double* partials;        // [gridDim.x][MAXQ][2]
+    double* partials;        // [CTA][MAXQ][2] (at least ny*nz CTAs)
     long long sstride;       // strided pass: element stride along the line
-    long long ostride;       // strided pass: stride of blockIdx.y
+    long long ostride;       // strided pass: stride of the outer index
     double t;                // Hamiltonian time (BEC quench)
     double dt, beta, lap_scale, DV, eps;
     double npart[2];
     double c_re, c_im;       // RK stage coefficient (stage 1..3 axpy; final uses c/6)
-    // Inputs staged in shared memory (slot s holds field stage_*[s] for the
-    // CTA's rows / lines); -1 = not staged.
-    int nstage;
-    int tma;                 // 1: bulk async copies (all alignments hold), 0: plain loads
-    const C* stage_ptr[MAXSTAGE];
-    int stage_kind[MAXSTAGE];
-    int stage_comp[MAXSTAGE];
-    int s_w[3], s_psi[2], s_v[2], s_a[2], s_k[2], s_xo[2];
 };
 
 // ---- shared-memory line addressing -----------------------------------------
@@ -103,12 +93,12 @@ struct PassArgs {
 __host__ __device__ constexpr int xpad(int L) { return L + (L >> 3); }
 template <typename C> struct RowAddr {      // X pass: S[b*xpad(L) + pos + pos/8]
     C* base;
-    __device__ __forceinline__ C* operator()(int pos) const { return base + pos + (pos >> 3); }
+    __device__ __forceinline__ C* operator()(unsigned pos) const { return base + (pos + (pos >> 3)); }
 };
 template <typename C> struct ColAddr {      // strided pass: S[pos*tx + b]
     C* base;
-    int tx;
-    __device__ __forceinline__ C* operator()(int pos) const { return base + pos * tx; }
+    unsigned tx;
+    __device__ __forceinline__ C* operator()(unsigned pos) const { return base + pos * tx; }
 };
 
 // ---- compensated FP64 reductions --------------------------------------------
@@ -275,6 +265,23 @@ __device__ __forceinline__ double2 rk_final(double2 old, double cr, double ci, d
     return make_double2(old.x + (cr * aX - ci * aY) / 6.0, old.y + (cr * aY + ci * aX) / 6.0);
 }
 
+// The same three stage updates in the field's own precision: the real-time
+// RK4 stages of the complex64 form run in FP32 (the complex128 form is the
+// FP64 arithmetic above, operation for operation).
+template <typename C, typename R>
+__device__ __forceinline__ C rk_axpy_r(C old, R cr, R ci, C h) {
+    return mk(old.x + (cr * h.x - ci * h.y), old.y + (cr * h.y + ci * h.x));
+}
+template <typename C, typename R>
+__device__ __forceinline__ C rk_final_r(C old, R cr, R ci, C k, C h) {
+    const R aX = k.x + h.x, aY = k.y + h.y;
+    return mk(old.x + (cr * aX - ci * aY) / (R)6, old.y + (cr * aY + ci * aX) / (R)6);
+}
+template <typename C>
+__device__ __forceinline__ C rk_kacc_r(C k, C h) {
+    return mk(k.x + 2 * h.x, k.y + 2 * h.y);
+}
+
 // ---- last-block finalize ------------------------------------------------------
 // Called by every block after its own reduction (thread 0 holds acc).
 template <typename R, int NQ>
@@ -285,10 +292,7 @@ __device__ void finalize_scalars(const PassArgs<R>& a, const double* S);
 
 // ---- kernels ----------------------------------------------------------------
 
-template <typename R, int L, int NF, int KIND>
-__global__ void __launch_bounds__(256, 1) k_xpass(PassArgs<R> a, int rows, int ntiles);
-
-template <typename R, int L, int NF>
-__global__ void __launch_bounds__(512, 1) k_spass(PassArgs<R> a, int ntx, int ntiles);
+// k_xpass<R, L, NF, KIND>(PassArgs<R> a, int rows) and
+// k_spass<R, L, NF>(PassArgs<R> a, int ntx): see gpe_kernels_impl.cuh.
 
 }  // namespace gpe

@@ -1,134 +1,60 @@
 // gpe_kernels_impl.cuh -- bodies of the axis-pass kernels (included by the
 // per-length instantiation units gpe_inst_*.cu).
+//
+// Every pass loads its lines straight from global memory into registers in
+// the FFT's register pattern (consecutive threads of a line hold consecutive
+// points, so each warp load is one or two 128-byte segments), runs the
+// Stockham passes with shared-memory exchanges, and stores from registers.
+// The x-inverse epilogue runs on the registers too: the other fields it needs
+// (psi, V, the RK4 stage fields) are loaded at the same positions.  One CTA
+// takes one tile; with no staging buffers the CTAs are small and many are
+// resident per SM, which is what hides the memory latency.
 #pragma once
 
 #include "gpe_kernels.cuh"
 
 namespace gpe {
 
-// ---- staged inputs ----------------------------------------------------------------
-// psi of component c at slot-local index li (prologue and epilogue source):
-// PRO_PIN as staged, PRO_CUR / PRO_A_SCALED times the lazy normalisation
-// factor of the current slot.
+// Programmatic dependent launch: the pass kernels are launched so that the
+// next pass's CTAs may be scheduled while the last CTAs of this pass run.
+// Each pass waits for the previous grid (and its memory) before touching
+// any field, then lets the following grid start launching.
+__device__ __forceinline__ void pass_prologue_sync() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Lazy normalisation factors of the current / previous heavy-ball slot.
 template <typename R>
-__device__ __forceinline__ typename Cx<R>::T psi_at(const PassArgs<R>& a, const typename Cx<R>::T* slots, int tile,
-                                                    int c, int li, int cur) {
-    typedef typename Cx<R>::T C;
-    const C x = slots[a.s_psi[c] * tile + li];
-    if (a.pro == PRO_PIN) return x;
-    const double s = a.sc->scale[cur][c];
+struct PsiScale {
+    double cur[2], old[2];
+};
+
+template <typename R>
+__device__ __forceinline__ PsiScale<R> load_scales(const PassArgs<R>& a, int cur) {
+    PsiScale<R> s;
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        s.cur[c] = a.sc->scale[cur][c];
+        s.old[c] = a.sc->scale[1 - cur][c];
+    }
+    return s;
+}
+
+template <typename C>
+__device__ __forceinline__ C scaled(C x, double s) {
     return from_d<C>(make_double2((double)x.x * s, (double)x.y * s));
 }
 
+// psi of component c at global index gi (prologue and epilogue source):
+// PRO_PIN as stored, PRO_CUR / PRO_A_SCALED times the lazy normalisation
+// factor of the current slot.
 template <typename R>
-__device__ __forceinline__ const typename Cx<R>::T* stage_source(const PassArgs<R>& a, int s, int cur) {
-    const int k = a.stage_kind[s], c = a.stage_comp[s];
-    if (k == SK_CUR) return a.buf[cur][c];
-    if (k == SK_OLD) return a.buf[1 - cur][c];
-    return a.stage_ptr[s];
-}
-
-// ---- tile staging pipeline ---------------------------------------------------------------
-// Inputs of a tile are copied asynchronously into one of two shared-memory
-// buffers while the CTA computes the previous tile.  x pass: one bulk copy
-// (TMA engine) per staged field when rows are 16-byte aligned, completing on
-// an mbarrier; strided pass (and unaligned rows): cp.async of 16-byte chunks
-// (8-byte elements when a chunk would straddle alignment) by all threads.
-
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
-// Copy nseg segments of seg elements (segment q: global g0 + q*gstride ->
-// slot offset q*sstride) of every staged field with cp.async; commits one group.
-template <typename R>
-__device__ __forceinline__ void issue_cp_async(const PassArgs<R>& a, typename Cx<R>::T* slots, int tile, long long g0,
-                                               int nseg, int seg, long long gstride, int sstride, int cur,
-                                               bool chunk16) {
-    typedef typename Cx<R>::T C;
-    const int ns = a.nstage;
-    if (chunk16) {
-        constexpr int EPC = 16 / sizeof(C);  // elements per 16-byte chunk
-        const int nch = seg / EPC;
-        if (nch > 0 && blockDim.x % nch == 0) {
-            // each thread keeps one chunk column j and walks segments q0, q0+qs, ...
-            const int j = threadIdx.x % nch, q0 = threadIdx.x / nch, qs = blockDim.x / nch;
-            for (int f = 0; f < ns; ++f) {
-                const C* src = stage_source(a, f, cur) + g0 + j * EPC;
-                C* dst = slots + (size_t)f * tile + j * EPC;
-                for (int q = q0; q < nseg; q += qs)
-                    cp_async16(dst + q * sstride, src + (unsigned)q * (unsigned)gstride);
-            }
-            cp_async_commit();
-            return;
-        }
-        const int total = ns * nseg * nch;
-        for (int k = threadIdx.x; k < total; k += blockDim.x) {
-            const int f = k / (nseg * nch);
-            const int r = k - f * (nseg * nch);
-            const int q = r / nch, j = r - q * nch;
-            cp_async16(slots + (size_t)f * tile + (size_t)q * sstride + j * EPC,
-                       stage_source(a, f, cur) + g0 + q * gstride + j * EPC);
-        }
-    } else {
-        const int total = ns * nseg * seg;
-        for (int k = threadIdx.x; k < total; k += blockDim.x) {
-            const int f = k / (nseg * seg);
-            const int r = k - f * (nseg * seg);
-            const int q = r / seg, j = r - q * seg;
-            C* d = slots + (size_t)f * tile + (size_t)q * sstride + j;
-            const C* sp = stage_source(a, f, cur) + g0 + q * gstride + j;
-            if (sizeof(C) == 16) cp_async16(d, sp);
-            else cp_async8(d, sp);
-        }
-    }
-    cp_async_commit();
-}
-
-// x pass: nvalid contiguous rows of L elements per staged field.
-template <typename R>
-__device__ __forceinline__ void issue_rows(const PassArgs<R>& a, typename Cx<R>::T* slots, int tile, long long g0,
-                                           int nelems, int cur, uint64_t* mbar) {
-    typedef typename Cx<R>::T C;
-    if (a.nstage == 0) return;
-    if (a.tma) {
-        if (threadIdx.x == 0) {
-            fence_proxy_async_smem();
-            const uint32_t bytes = (uint32_t)(nelems * sizeof(C));
-            mbar_arrive_expect_tx(mbar, bytes * (uint32_t)a.nstage);
-            for (int f = 0; f < a.nstage; ++f) bulk_g2s(slots + (size_t)f * tile, stage_source(a, f, cur) + g0, bytes, mbar);
-        }
-    } else {
-        issue_cp_async<R>(a, slots, tile, g0, 1, nelems, 0, 0, cur, false);
-    }
-}
-
-// Wait for the x-pass tile in buffer s (use count u); `more` = a later tile
-// was issued after this one.  Uniform across the CTA; false after a timeout.
-template <typename R>
-__device__ __forceinline__ bool wait_rows(const PassArgs<R>& a, uint64_t* mbar, uint32_t parity, bool more) {
-    if (a.nstage == 0) return true;
-    if (a.tma) {
-        const bool ok = mbar_wait_bounded(mbar, parity, 2000000000ull);
-        if (__syncthreads_or(!ok)) {
-            if (threadIdx.x == 0) {
-                a.sc->status = GPE_ERR_TIMEOUT;
-                a.sc->done = 1;
-            }
-            return false;
-        }
-        return true;
-    }
-    if (more) cp_async_wait_1();
-    else cp_async_wait_0();
-    __syncthreads();
-    return true;
+__device__ __forceinline__ typename Cx<R>::T load_psi(const PassArgs<R>& a, const PsiScale<R>& ps, int c, long long gi,
+                                                      int cur) {
+    if (a.pro == PRO_PIN) return a.pin[c][gi];
+    if (a.pro == PRO_CUR) return scaled(a.buf[cur][c][gi], ps.cur[c]);
+    return scaled(a.buf[0][c][gi], ps.cur[c]);
 }
 
 // ---- k-space multiply ---------------------------------------------------------
@@ -290,151 +216,263 @@ __device__ void reduce_and_finalize(const PassArgs<R>& a, DD (&acc)[NQ], DD* red
 }
 
 // ---- epilogue for one grid point ------------------------------------------------
-// v: the NF inverse-transformed fields at this point (kinetic part per psi
-// component, dipolar potential field last).  Inputs are read from the staged
-// slots at li, outputs written to global memory at gi.
-template <typename R, int NF, int EPI>
-__device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const HamCoef<R>& hc, const typename Cx<R>::T* v,
-                                               const typename Cx<R>::T* slots, int tile, int li, long long gi,
-                                               int cur, DD* acc) {
+// The epilogue of a chunk of points first loads every input it needs
+// (load_inputs), then computes and stores (epilogue_point).  Loading first
+// lets all loads of the chunk be in flight together: a load that followed a
+// store of the previous point could not be moved above it, because the state
+// buffers are updated in place (the stage state is read from and written to
+// the same array, each point by the thread that owns it).
+template <typename C>
+struct EpiIn {
+    C V[2], psi[2], k[2], p0[2], xo[2];
+};
+
+template <typename R, int EPI>
+__device__ __forceinline__ EpiIn<typename Cx<R>::T> load_inputs(const PassArgs<R>& a, const PsiScale<R>& ps,
+                                                                long long gi, int cur) {
+    typedef typename Cx<R>::T C;
+    EpiIn<C> in;
+    const int nc = a.ncomp;
+    if constexpr (EPI != EPI_STORE) {
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            if (c >= nc) continue;
+            in.V[c] = a.vext[c][gi];
+            if constexpr (EPI == EPI_RK) {
+                in.psi[c] = a.pin[c][gi];
+                if (a.stage > 1) {
+                    in.k[c] = a.kacc[c][gi];
+                    in.p0[c] = a.buf[0][c][gi];
+                }
+            } else if constexpr (EPI == EPI_HB) {
+                in.psi[c] = scaled(a.buf[cur][c][gi], ps.cur[c]);
+                in.xo[c] = a.buf[1 - cur][c][gi];
+            } else if constexpr (EPI == EPI_RKI) {
+                in.p0[c] = a.buf[0][c][gi];
+                if (a.stage > 1) {
+                    in.psi[c] = a.pin[c][gi];
+                    in.k[c] = a.kacc[c][gi];
+                }
+            } else {
+                in.psi[c] = load_psi<R>(a, ps, c, gi, cur);
+            }
+        }
+    }
+    return in;
+}
+
+// v: the NF inverse-transformed fields at global index gi (kinetic part per
+// psi component, dipolar potential field last); in: the loaded inputs.
+// For EPI_RK, nv receives the new state of each component (the value stored
+// in buf[1] for stages 1-3, in buf[0] for stage 4).
+template <typename R, int NF, int EPI, bool MAYRED = true>
+__device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const HamCoef<R>& hc, const PsiScale<R>& ps,
+                                               const typename Cx<R>::T* v, const EpiIn<typename Cx<R>::T>& in,
+                                               long long gi, int cur, DD* acc, typename Cx<R>::T* nv) {
     typedef typename Cx<R>::T C;
     const int nc = a.ncomp;
-    const int epi = (EPI >= 0) ? EPI : a.epi;
-    if (epi == EPI_STORE) {
+    if constexpr (EPI == EPI_STORE) {
 #pragma unroll
         for (int f = 0; f < NF; ++f) a.w[f][gi] = v[f];
         return;
-    }
-    C T[2], psi[2], V[2], hmu[2], hen[2];
-    const R phi = a.dens ? v[NF - 1].x : (R)0;
-#pragma unroll
-    for (int c = 0; c < 2; ++c) {
-        if (c < nc) {
-            T[c] = v[c];
-            V[c] = slots[a.s_v[c] * tile + li];
-        }
-    }
-    if (epi == EPI_RK) {
-        const int stage = a.stage;
-        const bool want_en = (stage == 4) && a.want_obs;
-#pragma unroll
-        for (int c = 0; c < 2; ++c)
-            if (c < nc) psi[c] = slots[a.s_psi[c] * tile + li];
-        ham_point<R, C>(a.ham, nc, hc, psi, T, V, phi, want_en, hmu, hen);
+    } else {
+        C T[2], psi[2], V[2], hmu[2], hen[2];
+        const R phi = a.dens ? v[NF - 1].x : (R)0;
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
-            if (c >= nc) continue;
-            const double2 h = to_d(hmu[c]);
-            if (stage == 1) {
-                a.kacc[c][gi] = hmu[c];
-                a.buf[1][c][gi] = from_d<C>(rk_axpy(to_d(psi[c]), a.c_re, a.c_im, h));
-            } else if (stage < 4) {
-                const double2 k = to_d(slots[a.s_k[c] * tile + li]);
-                a.kacc[c][gi] = from_d<C>(make_double2(k.x + 2.0 * h.x, k.y + 2.0 * h.y));
-                a.buf[1][c][gi] = from_d<C>(rk_axpy(to_d(slots[a.s_a[c] * tile + li]), a.c_re, a.c_im, h));
-            } else {
-                const C nv = from_d<C>(rk_final(to_d(slots[a.s_a[c] * tile + li]), a.c_re, a.c_im,
-                                                to_d(slots[a.s_k[c] * tile + li]), h));
-                a.buf[0][c][gi] = nv;
-                if (a.want_obs) {
-                    const double2 n = to_d(nv);
+            if (c < nc) {
+                T[c] = v[c];
+                V[c] = in.V[c];
+            }
+        }
+        if constexpr (EPI == EPI_RK) {
+            const int stage = a.stage;
+            const bool want_en = MAYRED && (stage == 4) && a.want_obs;
+#pragma unroll
+            for (int c = 0; c < 2; ++c)
+                if (c < nc) psi[c] = in.psi[c];
+            ham_point<R, C>(a.ham, nc, hc, psi, T, V, phi, want_en, hmu, hen);
+            const R cr = (R)a.c_re, ci = (R)a.c_im;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                if (c >= nc) continue;
+                const C hm = hmu[c];
+                if (stage == 1) {
+                    a.kacc[c][gi] = hm;
+                    nv[c] = rk_axpy_r(psi[c], cr, ci, hm);
+                    a.buf[1][c][gi] = nv[c];
+                } else if (stage < 4) {
+                    a.kacc[c][gi] = rk_kacc_r(in.k[c], hm);
+                    nv[c] = rk_axpy_r(in.p0[c], cr, ci, hm);
+                    a.buf[1][c][gi] = nv[c];
+                } else {
+                    nv[c] = rk_final_r(in.p0[c], cr, ci, in.k[c], hm);
+                    a.buf[0][c][gi] = nv[c];
+                    if (MAYRED && a.want_obs) {
+                        const double2 h = to_d(hm);
+                        const double2 n = to_d(nv[c]);
+                        const double2 he = to_d(hen[c]);
+                        acc[3 * c + 0] = dd_add(acc[3 * c + 0], n.x * n.x + n.y * n.y);
+                        acc[3 * c + 1] = dd_add(acc[3 * c + 1], n.x * h.x + n.y * h.y);
+                        acc[3 * c + 2] = dd_add(acc[3 * c + 2], n.x * he.x + n.y * he.y);
+                    }
+                }
+            }
+            return;
+        } else if constexpr (EPI == EPI_HB) {
+            // BECUpdatePsi (src/parallel.cu:294-302) on psi = s_cur*X_cur and
+            // psi_old = s_old*X_old; psi~ is written over X_old.
+#pragma unroll
+            for (int c = 0; c < 2; ++c)
+                if (c < nc) psi[c] = in.psi[c];
+            ham_point<R, C>(a.ham, nc, hc, psi, T, V, phi, true, hmu, hen);
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                if (c >= nc) continue;
+                const double so = ps.old[c];
+                const C xo = in.xo[c];
+                const double ox = (double)xo.x * so, oy = (double)xo.y * so;
+                const double mu = (nc == 1) ? 0 * a.sc->mu[0] : a.sc->mu[c];
+                const double dt = a.dt, beta = a.beta;
+                const double2 p = to_d(psi[c]);
+                const double2 h = to_d(hmu[c]);
+                const double2 nw = make_double2((1.0 + mu * dt) * p.x - dt * h.x + beta * (p.x - ox),
+                                                (1.0 + mu * dt) * p.y - dt * h.y + beta * (p.y - oy));
+                const C ns = from_d<C>(nw);
+                a.buf[1 - cur][c][gi] = ns;
+                const double2 n = to_d(ns);
+                const double2 he = to_d(hen[c]);
+                acc[3 * c + 0] = dd_add(acc[3 * c + 0], n.x * n.x + n.y * n.y);
+                acc[3 * c + 1] = dd_add(acc[3 * c + 1], n.x * h.x + n.y * h.y);
+                acc[3 * c + 2] = dd_add(acc[3 * c + 2], n.x * he.x + n.y * he.y);
+            }
+            return;
+        } else if constexpr (EPI == EPI_RKI) {
+            const int stage = a.stage;
+            double2 p0[2];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                if (c >= nc) continue;
+                const double s = ps.cur[c];
+                const C x = in.p0[c];
+                p0[c] = make_double2((double)x.x * s, (double)x.y * s);
+                psi[c] = (stage == 1) ? from_d<C>(p0[c]) : in.psi[c];
+            }
+            ham_point<R, C>(a.ham, nc, hc, psi, T, V, phi, stage == 1, hmu, hen);
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                if (c >= nc) continue;
+                const double2 h = to_d(hmu[c]);
+                if (stage == 1) {
+                    const double2 p = to_d(psi[c]);
                     const double2 he = to_d(hen[c]);
+                    acc[3 * c + 0] = dd_add(acc[3 * c + 0], p.x * p.x + p.y * p.y);
+                    acc[3 * c + 1] = dd_add(acc[3 * c + 1], p.x * h.x + p.y * h.y);
+                    acc[3 * c + 2] = dd_add(acc[3 * c + 2], p.x * he.x + p.y * he.y);
+                    a.kacc[c][gi] = hmu[c];
+                    a.buf[1][c][gi] = from_d<C>(rk_axpy(p0[c], a.c_re, a.c_im, h));
+                } else if (stage < 4) {
+                    const double2 k = to_d(in.k[c]);
+                    a.kacc[c][gi] = from_d<C>(make_double2(k.x + 2.0 * h.x, k.y + 2.0 * h.y));
+                    a.buf[1][c][gi] = from_d<C>(rk_axpy(p0[c], a.c_re, a.c_im, h));
+                } else {
+                    const C nv = from_d<C>(rk_final(p0[c], a.c_re, a.c_im, to_d(in.k[c]), h));
+                    a.buf[0][c][gi] = nv;
+                    const double2 n = to_d(nv);
                     acc[3 * c + 0] = dd_add(acc[3 * c + 0], n.x * n.x + n.y * n.y);
-                    acc[3 * c + 1] = dd_add(acc[3 * c + 1], n.x * h.x + n.y * h.y);
-                    acc[3 * c + 2] = dd_add(acc[3 * c + 2], n.x * he.x + n.y * he.y);
+                }
+            }
+            return;
+        } else {
+            // EPI_APPLYH / EPI_OBS
+#pragma unroll
+            for (int c = 0; c < 2; ++c)
+                if (c < nc) psi[c] = in.psi[c];
+            ham_point<R, C>(a.ham, nc, hc, psi, T, V, phi, true, hmu, hen);
+            if constexpr (EPI == EPI_APPLYH) {
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    if (c >= nc) continue;
+                    if (a.out[2 * c]) a.out[2 * c][gi] = hmu[c];
+                    if (a.out[2 * c + 1]) a.out[2 * c + 1][gi] = hen[c];
+                }
+                return;
+            } else {
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    if (c >= nc) continue;
+                    const double2 p = to_d(psi[c]), h = to_d(hmu[c]), he = to_d(hen[c]);
+                    acc[3 * c + 0] = dd_add(acc[3 * c + 0], p.x * p.x + p.y * p.y);
+                    acc[3 * c + 1] = dd_add(acc[3 * c + 1], p.x * h.x + p.y * h.y);
+                    acc[3 * c + 2] = dd_add(acc[3 * c + 2], p.x * he.x + p.y * he.y);
                 }
             }
         }
-        return;
     }
-    if (epi == EPI_HB) {
-        // BECUpdatePsi (src/parallel.cu:294-302) on psi = s_cur*X_cur and
-        // psi_old = s_old*X_old; psi~ is written over X_old.
+}
+
+// Epilogue of E points (register e at line position pos(e)): inputs of a
+// chunk of EC points are loaded first, then the chunk is computed and stored.
+// FUSE: v[f][e] is replaced by the new RK state of component f (and, for the
+// dipolar density field, its |psi|^2), ready for the forward x transform.
+template <typename R, int NF, int EPI, bool MAYRED, int L, int E, int T, int Rr, bool FUSE = false>
+__device__ __forceinline__ void epilogue_line(const PassArgs<R>& a, const HamCoef<R>& hc, const PsiScale<R>& ps,
+                                              typename Cx<R>::T (&v)[NF][E], long long g0, int cur, DD* acc) {
+    typedef typename Cx<R>::T C;
+    constexpr int EC0 = NF > 1 ? 1 : 2;
+    constexpr int EC = (E % EC0 == 0) ? EC0 : ((E % 4 == 0) ? 4 : ((E % 2 == 0) ? 2 : 1));
 #pragma unroll
-        for (int c = 0; c < 2; ++c)
-            if (c < nc) psi[c] = psi_at<R>(a, slots, tile, c, li, cur);
-        ham_point<R, C>(a.ham, nc, hc, psi, T, V, phi, true, hmu, hen);
+    for (int e0 = 0; e0 < E; e0 += EC) {
+        EpiIn<C> in[EC];
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            if (c >= nc) continue;
-            const double so = a.sc->scale[1 - cur][c];
-            const C xo = slots[a.s_xo[c] * tile + li];
-            const double ox = (double)xo.x * so, oy = (double)xo.y * so;
-            const double mu = (nc == 1) ? 0 * a.sc->mu[0] : a.sc->mu[c];
-            const double dt = a.dt, beta = a.beta;
-            const double2 p = to_d(psi[c]);
-            const double2 h = to_d(hmu[c]);
-            const double2 nw = make_double2((1.0 + mu * dt) * p.x - dt * h.x + beta * (p.x - ox),
-                                            (1.0 + mu * dt) * p.y - dt * h.y + beta * (p.y - oy));
-            const C ns = from_d<C>(nw);
-            a.buf[1 - cur][c][gi] = ns;
-            const double2 n = to_d(ns);
-            const double2 he = to_d(hen[c]);
-            acc[3 * c + 0] = dd_add(acc[3 * c + 0], n.x * n.x + n.y * n.y);
-            acc[3 * c + 1] = dd_add(acc[3 * c + 1], n.x * h.x + n.y * h.y);
-            acc[3 * c + 2] = dd_add(acc[3 * c + 2], n.x * he.x + n.y * he.y);
-        }
-        return;
-    }
-    if (epi == EPI_RKI) {
-        const int stage = a.stage;
-        double2 p0[2];
+        for (int j = 0; j < EC; ++j) in[j] = load_inputs<R, EPI>(a, ps, g0 + reg_off<L, E, T, Rr>(e0 + j), cur);
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            if (c >= nc) continue;
-            const double s = a.sc->scale[cur][c];
-            const C x = slots[a.s_a[c] * tile + li];
-            p0[c] = make_double2((double)x.x * s, (double)x.y * s);
-            psi[c] = (stage == 1) ? from_d<C>(p0[c]) : slots[a.s_psi[c] * tile + li];
-        }
-        ham_point<R, C>(a.ham, nc, hc, psi, T, V, phi, stage == 1, hmu, hen);
+        for (int j = 0; j < EC; ++j) {
+            C tmp[NF];
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            if (c >= nc) continue;
-            const double2 h = to_d(hmu[c]);
-            if (stage == 1) {
-                const double2 p = to_d(psi[c]);
-                const double2 he = to_d(hen[c]);
-                acc[3 * c + 0] = dd_add(acc[3 * c + 0], p.x * p.x + p.y * p.y);
-                acc[3 * c + 1] = dd_add(acc[3 * c + 1], p.x * h.x + p.y * h.y);
-                acc[3 * c + 2] = dd_add(acc[3 * c + 2], p.x * he.x + p.y * he.y);
-                a.kacc[c][gi] = hmu[c];
-                a.buf[1][c][gi] = from_d<C>(rk_axpy(p0[c], a.c_re, a.c_im, h));
-            } else if (stage < 4) {
-                const double2 k = to_d(slots[a.s_k[c] * tile + li]);
-                a.kacc[c][gi] = from_d<C>(make_double2(k.x + 2.0 * h.x, k.y + 2.0 * h.y));
-                a.buf[1][c][gi] = from_d<C>(rk_axpy(p0[c], a.c_re, a.c_im, h));
-            } else {
-                const C nv = from_d<C>(rk_final(p0[c], a.c_re, a.c_im, to_d(slots[a.s_k[c] * tile + li]), h));
-                a.buf[0][c][gi] = nv;
-                const double2 n = to_d(nv);
-                acc[3 * c + 0] = dd_add(acc[3 * c + 0], n.x * n.x + n.y * n.y);
+            for (int f = 0; f < NF; ++f) tmp[f] = v[f][e0 + j];
+            C nv[2];
+            epilogue_point<R, NF, EPI, MAYRED>(a, hc, ps, tmp, in[j], g0 + reg_off<L, E, T, Rr>(e0 + j), cur, acc,
+                                               nv);
+            if constexpr (FUSE) {
+                const int npsi = NF - a.dens;
+#pragma unroll
+                for (int f = 0; f < NF; ++f) {
+                    if (f < npsi) v[f][e0 + j] = nv[f < 2 ? f : 1];
+                    else v[f][e0 + j] = mk(nv[0].x * nv[0].x + nv[0].y * nv[0].y, (R)0);
+                }
             }
         }
-        return;
     }
-    // EPI_APPLYH / EPI_OBS
-#pragma unroll
-    for (int c = 0; c < 2; ++c)
-        if (c < nc) psi[c] = psi_at<R>(a, slots, tile, c, li, cur);
-    ham_point<R, C>(a.ham, nc, hc, psi, T, V, phi, true, hmu, hen);
-    if (epi == EPI_APPLYH) {
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            if (c >= nc) continue;
-            if (a.out[2 * c]) a.out[2 * c][gi] = hmu[c];
-            if (a.out[2 * c + 1]) a.out[2 * c + 1][gi] = hen[c];
+}
+
+// Epilogue of a line with the op of the kernel role.
+template <typename R, int NF, int KIND, int L, int E, int T, int Rr>
+__device__ __forceinline__ void epilogue_dispatch(const PassArgs<R>& a, const HamCoef<R>& hc, const PsiScale<R>& ps,
+                                                  typename Cx<R>::T (&v)[NF][E], long long g0, int cur, DD* acc) {
+#define GPE_EPI(OP, RED) epilogue_line<R, NF, OP, RED, L, E, T, Rr>(a, hc, ps, v, g0, cur, acc)
+    if constexpr (KIND == XK_STORE) GPE_EPI(EPI_STORE, false);
+    else if constexpr (KIND == XK_RK) GPE_EPI(EPI_RK, false);
+    else if constexpr (KIND == XK_RKF)
+        epilogue_line<R, NF, EPI_RK, false, L, E, T, Rr, true>(a, hc, ps, v, g0, cur, acc);
+    else if constexpr (KIND == XK_RKO) GPE_EPI(EPI_RK, true);
+    else if constexpr (KIND == XK_HB) GPE_EPI(EPI_HB, true);
+    else if constexpr (KIND == XK_RKI) GPE_EPI(EPI_RKI, true);
+    else if constexpr (KIND == XK_AH) {
+        // the apply-H kernel serves both EPI_APPLYH and EPI_OBS
+        if (a.epi == EPI_OBS) GPE_EPI(EPI_OBS, true);
+        else GPE_EPI(EPI_APPLYH, true);
+    } else {  // XK_FULL: run-time op
+        switch (a.epi) {
+            case EPI_STORE: GPE_EPI(EPI_STORE, false); break;
+            case EPI_RK: GPE_EPI(EPI_RK, true); break;
+            case EPI_HB: GPE_EPI(EPI_HB, true); break;
+            case EPI_RKI: GPE_EPI(EPI_RKI, true); break;
+            case EPI_APPLYH: GPE_EPI(EPI_APPLYH, true); break;
+            default: GPE_EPI(EPI_OBS, true); break;
         }
-        return;
     }
-#pragma unroll
-    for (int c = 0; c < 2; ++c) {
-        if (c >= nc) continue;
-        const double2 p = to_d(psi[c]), h = to_d(hmu[c]), he = to_d(hen[c]);
-        acc[3 * c + 0] = dd_add(acc[3 * c + 0], p.x * p.x + p.y * p.y);
-        acc[3 * c + 1] = dd_add(acc[3 * c + 1], p.x * h.x + p.y * h.y);
-        acc[3 * c + 2] = dd_add(acc[3 * c + 2], p.x * he.x + p.y * he.y);
-    }
+#undef GPE_EPI
 }
 
 template <typename R>
@@ -443,41 +481,66 @@ __device__ __forceinline__ bool epi_reduces(const PassArgs<R>& a) {
            (a.epi == EPI_RKI && (a.stage == 1 || a.stage == 4));
 }
 
+// Kernel roles that may reduce (the others never touch the partials).
+template <int KIND>
+__host__ __device__ constexpr bool kind_reduces() {
+    return KIND == XK_RKO || KIND == XK_HB || KIND == XK_RKI || KIND == XK_AH || KIND == XK_FULL;
+}
+
+// Resident CTAs per SM the launch bounds ask for: complex64 lines of up to 8
+// values per thread fit three 256-thread CTAs; complex128 or longer register
+// arrays, two; two fields and long arrays, one.
+template <typename R, int L, int NF>
+__host__ __device__ constexpr int pass_min_blocks() {
+    constexpr int E = Plan<L>::E;
+    constexpr int w = (int)sizeof(R) / 4 * E * NF;  // 32-bit words of line values per thread / 2
+    return w <= 8 ? 3 : (w <= 16 ? 2 : 1);
+}
+
 // ---- X pass -----------------------------------------------------------------------
-// One tile = `rows` rows of the x axis (T threads per row).  Persistent CTAs
-// loop over tiles with the inputs of the next tile in flight.  Shared memory:
-// two buffers of a.nstage slots of rows*L elements, then the FFT exchange
-// buffer of rows*L elements.
+// One CTA = `rows` consecutive rows of the x axis, T threads per row.  Shared
+// memory: one padded exchange row per line (rows * xpad(L) elements).
+// Roles with the FP64 reductions hold more live values: one CTA fewer.
 template <typename R, int L, int NF, int KIND>
-__device__ __forceinline__ void xpass_tile(const PassArgs<R>& a, const HamCoef<R>& hc, const typename Cx<R>::T* slots,
-                                           typename Cx<R>::T* X, int tile, int row0, int cur, DD* acc) {
+__host__ __device__ constexpr int xpass_min_blocks() {
+    return kind_reduces<KIND>() && pass_min_blocks<R, L, NF>() > 1 ? pass_min_blocks<R, L, NF>() - 1
+                                                                    : pass_min_blocks<R, L, NF>();
+}
+
+template <typename R, int L, int NF, int KIND>
+__global__ void __launch_bounds__(256, (xpass_min_blocks<R, L, NF, KIND>())) k_xpass(PassArgs<R> a, int rows) {
     typedef typename Cx<R>::T C;
     constexpr int E = Plan<L>::E;
     constexpr int T = Plan<L>::T;
     constexpr int RinF = Plan<L>::in_radix(false);
     constexpr int RoutF = Plan<L>::out_radix(false);
-    const int b = threadIdx.x / T, t = threadIdx.x % T;
-    const bool valid = row0 + b < a.nrows;
-    const long long gbase = (long long)(row0 + (valid ? b : 0)) * L;
-    const int lbase = b * L;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    pass_prologue_sync();
+    if (a.check_done && a.sc->done) return;
+
+    C* X = reinterpret_cast<C*>(smem_raw);
+    const unsigned b = threadIdx.x / T, t = threadIdx.x % T;
+    const int row = blockIdx.x * rows + (int)b;
+    const bool valid = row < a.nrows;
+    // g0 + reg_off(e): global index of register e of this thread's line
+    const long long g0 = (long long)(valid ? row : 0) * L + t;
     const RowAddr<C> addr{X + b * xpad(L)};
-    constexpr int EPI = (KIND == XK_STORE) ? EPI_STORE
-                      : (KIND == XK_RK || KIND == XK_RKO) ? EPI_RK
-                      : (KIND == XK_HB)    ? EPI_HB
-                      : (KIND == XK_RKI)   ? EPI_RKI
-                      : (KIND == XK_AH)    ? EPI_APPLYH
-                                           : -1;
+    const int cur = a.sc->cur_slot;
+    const PsiScale<R> ps = load_scales<R>(a, cur);
+    DD acc[MAXQ];
+#pragma unroll
+    for (int q = 0; q < MAXQ; ++q) acc[q] = DD{0.0, 0.0};
     C v[NF][E];
 
     if constexpr (KIND == XK_FWD || KIND == XK_FULL) {
         const int npsi = NF - a.dens;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const int li = lbase + reg_pos<L, E, T, RinF>(t, e);
+            const long long gi = g0 + reg_off<L, E, T, RinF>(e);
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
                 if (f < npsi) {
-                    v[f][e] = valid ? psi_at<R>(a, slots, tile, f, li, cur) : mk((R)0, (R)0);
+                    v[f][e] = valid ? load_psi<R>(a, ps, f, gi, cur) : mk((R)0, (R)0);
                 } else {
                     const C p = v[0][e];
                     v[f][e] = mk(p.x * p.x + p.y * p.y, (R)0);
@@ -490,149 +553,107 @@ __device__ __forceinline__ void xpass_tile(const PassArgs<R>& a, const HamCoef<R
             if (valid) {
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
-                    const long long gi = gbase + reg_pos<L, E, T, RoutF>(t, e);
+                    const long long gi = g0 + reg_off<L, E, T, RoutF>(e);
 #pragma unroll
                     for (int f = 0; f < NF; ++f) a.w[f][gi] = v[f][e];
                 }
             }
             return;
-        }
-        // XM_FULL: x is the only transformed axis.
-        const int row = row0 + b;
-        const int iy = row % a.ny, iz = row / a.ny;
+        } else {
+            // x is the only transformed axis: k-space multiply here.
+            const int iy = row % a.ny, iz = row / a.ny;
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const int pos = reg_pos<L, E, T, RoutF>(t, e);
-            C tmp[NF];
+            for (int e = 0; e < E; ++e) {
+                const int pos = reg_pos<L, E, T, RoutF>((int)t, e);
+                C tmp[NF];
 #pragma unroll
-            for (int f = 0; f < NF; ++f) tmp[f] = v[f][e];
-            if (valid) spec_point<R, NF>(a, tmp, pos, iy, iz, gbase + pos);
+                for (int f = 0; f < NF; ++f) tmp[f] = v[f][e];
+                if (valid) spec_point<R, NF>(a, tmp, pos, iy, iz, g0 + reg_off<L, E, T, RoutF>(e));
 #pragma unroll
-            for (int f = 0; f < NF; ++f) v[f][e] = tmp[f];
+                for (int f = 0; f < NF; ++f) v[f][e] = tmp[f];
+            }
         }
     } else {
-        // XM_INV: registers in the inverse input pattern, from the staged W slots.
+        // inverse input pattern straight from the transformed fields
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const int li = lbase + reg_pos<L, E, T, RoutF>(t, e);
+            const long long gi = g0 + reg_off<L, E, T, RoutF>(e);
 #pragma unroll
-            for (int f = 0; f < NF; ++f) v[f][e] = valid ? slots[a.s_w[f] * tile + li] : mk((R)0, (R)0);
+            for (int f = 0; f < NF; ++f) v[f][e] = valid ? a.w[f][gi] : mk((R)0, (R)0);
         }
     }
-    // Inverse transform of each field; the results go to the exchange
-    // buffers (one per field, natural order) so that the epilogue can walk the
-    // points with consecutive threads on consecutive points and few live
-    // registers.
-    const int rows = blockDim.x / T;
+    if constexpr (KIND != XK_FWD) {
+        const HamCoef<R> hc = make_coef<R>(a);
 #pragma unroll
-    for (int f = 0; f < NF; ++f) {
-        line_fft_inv<L>(v[f], RowAddr<C>{X + (size_t)f * rows * xpad(L) + b * xpad(L)}, a.tw, t);
-        __syncthreads();
+        for (int f = 0; f < NF; ++f) line_fft_inv<L>(v[f], addr, a.tw, t);
+        if (valid) epilogue_dispatch<R, NF, KIND, L, E, T, RinF>(a, hc, ps, v, g0, cur, acc);
+        if constexpr (KIND == XK_RKF) {
+            // next stage's x-forward pass on the state just written (in place on w)
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const int pos = reg_pos<L, E, T, RinF>(t, e);
-            X[(size_t)f * rows * xpad(L) + b * xpad(L) + pos + (pos >> 3)] = v[f][e];
+            for (int f = 0; f < NF; ++f) line_fft_fwd<L>(v[f], addr, a.tw, t);
+            if (valid) {
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const long long gi = g0 + reg_off<L, E, T, RoutF>(e);
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) a.w[f][gi] = v[f][e];
+                }
+            }
+        }
+        if constexpr (kind_reduces<KIND>()) {
+            if (epi_reduces(a)) {
+                __shared__ DD red[32 * MAXQ];
+                reduce_and_finalize<R, MAXQ>(a, acc, red);
+            }
         }
     }
-    __syncthreads();
-    const int nvalid = min(rows, a.nrows - row0);
-    for (int i = threadIdx.x; i < nvalid * L; i += blockDim.x) {
-        const int bb = i / L, pos = i - bb * L;
-        C tmp[NF];
-#pragma unroll
-        for (int f = 0; f < NF; ++f) tmp[f] = X[(size_t)f * rows * xpad(L) + bb * xpad(L) + pos + (pos >> 3)];
-        const int li = bb * L + pos;
-        const long long gi = (long long)(row0 + bb) * L + pos;
-        if constexpr (EPI == EPI_APPLYH) {
-            // the apply-H kernel serves both EPI_APPLYH and EPI_OBS
-            if (a.epi == EPI_OBS) epilogue_point<R, NF, EPI_OBS>(a, hc, tmp, slots, tile, li, gi, cur, acc);
-            else epilogue_point<R, NF, EPI_APPLYH>(a, hc, tmp, slots, tile, li, gi, cur, acc);
-        } else {
-            epilogue_point<R, NF, EPI>(a, hc, tmp, slots, tile, li, gi, cur, acc);
-        }
-    }
-}
-
-template <typename R, int L, int NF, int KIND>
-__global__ void __launch_bounds__(256, 1) k_xpass(PassArgs<R> a, int rows, int ntiles) {
-    typedef typename Cx<R>::T C;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ DD red[32 * MAXQ];
-    __shared__ __align__(8) uint64_t mbar[2];
-    if (a.check_done && a.sc->done) return;
-
-    const int tile = rows * L;
-    const int ns = a.nstage;
-    C* bufs = reinterpret_cast<C*>(smem_raw);
-    C* X = bufs + (size_t)2 * ns * tile;
-    const int cur = a.sc->cur_slot;
-    const HamCoef<R> hc = make_coef<R>(a);
-    DD acc[MAXQ];
-#pragma unroll
-    for (int q = 0; q < MAXQ; ++q) acc[q] = DD{0.0, 0.0};
-    if (threadIdx.x == 0 && a.tma) {
-        mbar_init(&mbar[0], 1);
-        mbar_init(&mbar[1], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-    auto nrow = [&](int tl) { return min(rows, a.nrows - tl * rows); };
-    int tl = blockIdx.x;
-    if (tl < ntiles) issue_rows<R>(a, bufs, tile, (long long)tl * rows * L, nrow(tl) * L, cur, &mbar[0]);
-    if (tl + (int)gridDim.x < ntiles)
-        issue_rows<R>(a, bufs + (size_t)ns * tile, tile, (long long)(tl + gridDim.x) * rows * L,
-                      nrow(tl + gridDim.x) * L, cur, &mbar[1]);
-    for (int i = 0; tl < ntiles; ++i, tl += gridDim.x) {
-        const int sb = i & 1;
-        C* slots = bufs + (size_t)sb * ns * tile;
-        if (!wait_rows<R>(a, &mbar[sb], (uint32_t)((i >> 1) & 1), tl + (int)gridDim.x < ntiles)) return;
-        xpass_tile<R, L, NF, KIND>(a, hc, slots, X, tile, tl * rows, cur, acc);
-        __syncthreads();
-        const int nx2 = tl + 2 * (int)gridDim.x;
-        if (nx2 < ntiles) issue_rows<R>(a, slots, tile, (long long)nx2 * rows * L, nrow(nx2) * L, cur, &mbar[sb]);
-    }
-    // Only the epilogue-bearing passes reduce (the forward pass carries the
-    // chain's epilogue op but runs no epilogue).
-    if constexpr (KIND != XK_FWD && KIND != XK_STORE && KIND != XK_RK)
-        if (epi_reduces(a)) reduce_and_finalize<R, MAXQ>(a, acc, red);
 }
 
 // ---- strided pass -----------------------------------------------------------------
-// One tile = tx consecutive x values x the whole line along y or z
-// (ntx = ceil(nx/tx) tiles per outer index).  Shared memory: two buffers of
-// a.nstage (= NF) W slots of L*tx elements ([pos][b]), then the exchange buffer.
+// One CTA = tx consecutive x values x the whole line along y or z, for one
+// outer index (blockIdx.x = outer * ntx + x block).  Thread (b, t) = (line
+// b of the tile, thread t of the line); b is the fast index so that a warp
+// loads tx consecutive x values per line position.  Shared memory: the
+// exchange buffer S[pos * tx + b].
 template <typename R, int L, int NF>
-__device__ __forceinline__ void spass_tile(const PassArgs<R>& a, const typename Cx<R>::T* slots,
-                                           typename Cx<R>::T* X, int tile, int x0, int outer) {
+__global__ void __launch_bounds__(256, (pass_min_blocks<R, L, NF>())) k_spass(PassArgs<R> a, int ntx) {
     typedef typename Cx<R>::T C;
     constexpr int E = Plan<L>::E;
     constexpr int T = Plan<L>::T;
     constexpr int RinF = Plan<L>::in_radix(false);
     constexpr int RoutF = Plan<L>::out_radix(false);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    pass_prologue_sync();
+    if (a.check_done && a.sc->done) return;
+
+    C* X = reinterpret_cast<C*>(smem_raw);
     const int tx = a.tx;
-    const int b = threadIdx.x % tx, t = threadIdx.x / tx;
-    const bool valid = x0 + b < a.nx;
-    const long long base0 = (long long)outer * a.ostride + x0;
+    const int xb = blockIdx.x % ntx, outer = blockIdx.x / ntx;
+    const int x0 = xb * tx;
+    const unsigned b = threadIdx.x % tx, t = threadIdx.x / tx;
+    const bool valid = x0 + (int)b < a.nx;
     const long long ss = a.sstride;
-    const ColAddr<C> addr{X + b, tx};
+    // g0 + reg_off(e) * ss: global index of register e of this thread's line
+    const long long g0 = (long long)outer * a.ostride + x0 + (valid ? b : 0) + (long long)t * ss;
+    const ColAddr<C> addr{X + b, (unsigned)tx};
     const int mode = a.mode;
     C v[NF][E];
 
     if (mode == SM_INV) {
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const int li = reg_pos<L, E, T, RoutF>(t, e) * tx + b;
+            const long long gi = g0 + (long long)reg_off<L, E, T, RoutF>(e) * ss;
 #pragma unroll
-            for (int f = 0; f < NF; ++f) v[f][e] = valid ? slots[a.s_w[f] * tile + li] : mk((R)0, (R)0);
+            for (int f = 0; f < NF; ++f) v[f][e] = valid ? a.w[f][gi] : mk((R)0, (R)0);
         }
 #pragma unroll
         for (int f = 0; f < NF; ++f) line_fft_inv<L>(v[f], addr, a.tw, t);
     } else {
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const int li = reg_pos<L, E, T, RinF>(t, e) * tx + b;
+            const long long gi = g0 + (long long)reg_off<L, E, T, RinF>(e) * ss;
 #pragma unroll
-            for (int f = 0; f < NF; ++f) v[f][e] = valid ? slots[a.s_w[f] * tile + li] : mk((R)0, (R)0);
+            for (int f = 0; f < NF; ++f) v[f][e] = valid ? a.w[f][gi] : mk((R)0, (R)0);
         }
 #pragma unroll
         for (int f = 0; f < NF; ++f) line_fft_fwd<L>(v[f], addr, a.tw, t);
@@ -640,7 +661,7 @@ __device__ __forceinline__ void spass_tile(const PassArgs<R>& a, const typename 
             if (valid) {
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
-                    const long long gi = base0 + b + (long long)reg_pos<L, E, T, RoutF>(t, e) * ss;
+                    const long long gi = g0 + (long long)reg_off<L, E, T, RoutF>(e) * ss;
 #pragma unroll
                     for (int f = 0; f < NF; ++f) a.w[f][gi] = v[f][e];
                 }
@@ -651,14 +672,14 @@ __device__ __forceinline__ void spass_tile(const PassArgs<R>& a, const typename 
         if (a.spec != SPEC_NONE) {
 #pragma unroll
             for (int e = 0; e < E; ++e) {
-                const int pos = reg_pos<L, E, T, RoutF>(t, e);
+                const int pos = reg_pos<L, E, T, RoutF>((int)t, e);
                 C tmp[NF];
 #pragma unroll
                 for (int f = 0; f < NF; ++f) tmp[f] = v[f][e];
                 if (valid) {
                     const int iy = (a.sax == 2) ? outer : pos;
                     const int iz = (a.sax == 2) ? pos : outer;
-                    spec_point<R, NF>(a, tmp, x0 + b, iy, iz, base0 + b + (long long)pos * ss);
+                    spec_point<R, NF>(a, tmp, x0 + (int)b, iy, iz, g0 + (long long)reg_off<L, E, T, RoutF>(e) * ss);
                 }
 #pragma unroll
                 for (int f = 0; f < NF; ++f) v[f][e] = tmp[f];
@@ -670,78 +691,49 @@ __device__ __forceinline__ void spass_tile(const PassArgs<R>& a, const typename 
     if (valid) {
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const long long gi = base0 + b + (long long)reg_pos<L, E, T, RinF>(t, e) * ss;
+            const long long gi = g0 + (long long)reg_off<L, E, T, RinF>(e) * ss;
 #pragma unroll
             for (int f = 0; f < NF; ++f) a.w[f][gi] = v[f][e];
         }
     }
 }
 
-template <typename R, int L, int NF>
-__global__ void __launch_bounds__(512, 1) k_spass(PassArgs<R> a, int ntx, int ntiles) {
-    typedef typename Cx<R>::T C;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    if (a.check_done && a.sc->done) return;
-
-    const int tx = a.tx;
-    const int tile = L * tx;
-    const int ns = a.nstage;
-    C* bufs = reinterpret_cast<C*>(smem_raw);
-    C* X = bufs + (size_t)2 * ns * tile;
-    const bool chunk16 = a.tma != 0;
-    auto issue = [&](int tl, C* slots) {
-        const int xb = tl % ntx, outer = tl / ntx;
-        const int x0 = xb * tx;
-        const int nxv = min(tx, a.nx - x0);
-        issue_cp_async<R>(a, slots, tile, (long long)outer * a.ostride + x0, L, nxv, a.sstride, tx, 0, chunk16);
-    };
-    int tl = blockIdx.x;
-    if (tl < ntiles) issue(tl, bufs);
-    if (tl + (int)gridDim.x < ntiles) issue(tl + gridDim.x, bufs + (size_t)ns * tile);
-    for (int i = 0; tl < ntiles; ++i, tl += gridDim.x) {
-        const int sb = i & 1;
-        C* slots = bufs + (size_t)sb * ns * tile;
-        if (tl + (int)gridDim.x < ntiles) cp_async_wait_1();
-        else cp_async_wait_0();
-        __syncthreads();
-        spass_tile<R, L, NF>(a, slots, X, tile, (tl % ntx) * tx, tl / ntx);
-        __syncthreads();
-        const int nx2 = tl + 2 * (int)gridDim.x;
-        if (nx2 < ntiles) issue(nx2, slots);
-    }
-}
-
 // ---- launchers ----------------------------------------------------------------------
-inline int sm_count() {
-    static int n = 0;
-    if (!n) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 1;
-    }
-    return n;
+// rows: rows per CTA (x pass); smem: exchange buffer bytes; both chosen by the host.
+// Launch with programmatic stream serialization (see pass_prologue_sync).
+template <typename K, typename... Args>
+cudaError_t launch_pass(K kernel, unsigned grid, unsigned threads, size_t smem, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
-// rows: rows per tile (x pass), smem bytes per CTA, both chosen by the host.
-// The grid is persistent: min(tiles, resident CTAs).
+// Exchange buffers above the default 48 KB (short lines with E = 12..24
+// values per thread and 256 rows, complex128) need the opt-in attribute.
+template <typename K>
+cudaError_t allow_smem(K kernel, size_t smem, bool& done) {
+    if (smem <= 48 * 1024 || done) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    if (e == cudaSuccess) done = true;
+    return e;
+}
+
 template <typename R, int L, int NF, int KIND>
 cudaError_t launch_xpass_kind(const PassArgs<R>& a, int rows, size_t smem, cudaStream_t st) {
     static bool attr = false;
-    if (!attr) {
-        cudaError_t e =
-            cudaFuncSetAttribute(k_xpass<R, L, NF, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    cudaError_t e = allow_smem(k_xpass<R, L, NF, KIND>, smem, attr);
+    if (e != cudaSuccess) return e;
     const int threads = rows * Plan<L>::T;
-    const int ntiles = (a.nrows + rows - 1) / rows;
-    int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_xpass<R, L, NF, KIND>, threads, smem);
-    if (occ < 1) occ = 1;
-    const int grid = min(ntiles, occ * sm_count());
-    k_xpass<R, L, NF, KIND><<<grid, threads, smem, st>>>(a, rows, ntiles);
-    return cudaGetLastError();
+    const int grid = (a.nrows + rows - 1) / rows;
+    return launch_pass(k_xpass<R, L, NF, KIND>, (unsigned)grid, (unsigned)threads, smem, st, a, rows);
 }
 
 // Kernel role from the pass mode and epilogue op.
@@ -761,11 +753,13 @@ template <typename R, int L, int NF>
 cudaError_t launch_xpass(const PassArgs<R>& a, int rows, size_t smem, cudaStream_t st) {
     int kind = xkind_of(a.mode, a.epi);
     if (kind == XK_RK && a.want_obs && a.stage == 4) kind = XK_RKO;
+    else if (kind == XK_RK && a.fuse_fwd) kind = XK_RKF;
     switch (kind) {
         case XK_FWD: return launch_xpass_kind<R, L, NF, XK_FWD>(a, rows, smem, st);
         case XK_STORE: return launch_xpass_kind<R, L, NF, XK_STORE>(a, rows, smem, st);
         case XK_RK: return launch_xpass_kind<R, L, NF, XK_RK>(a, rows, smem, st);
         case XK_RKO: return launch_xpass_kind<R, L, NF, XK_RKO>(a, rows, smem, st);
+        case XK_RKF: return launch_xpass_kind<R, L, NF, XK_RKF>(a, rows, smem, st);
         case XK_HB: return launch_xpass_kind<R, L, NF, XK_HB>(a, rows, smem, st);
         case XK_RKI: return launch_xpass_kind<R, L, NF, XK_RKI>(a, rows, smem, st);
         case XK_AH: return launch_xpass_kind<R, L, NF, XK_AH>(a, rows, smem, st);
@@ -776,20 +770,11 @@ cudaError_t launch_xpass(const PassArgs<R>& a, int rows, size_t smem, cudaStream
 template <typename R, int L, int NF>
 cudaError_t launch_spass(const PassArgs<R>& a, int nouter, size_t smem, cudaStream_t st) {
     static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_spass<R, L, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    cudaError_t e = allow_smem(k_spass<R, L, NF>, smem, attr);
+    if (e != cudaSuccess) return e;
     const int threads = a.tx * Plan<L>::T;
     const int ntx = (a.nx + a.tx - 1) / a.tx;
-    const int ntiles = ntx * nouter;
-    int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_spass<R, L, NF>, threads, smem);
-    if (occ < 1) occ = 1;
-    const int grid = min(ntiles, occ * sm_count());
-    k_spass<R, L, NF><<<grid, threads, smem, st>>>(a, ntx, ntiles);
-    return cudaGetLastError();
+    return launch_pass(k_spass<R, L, NF>, (unsigned)(ntx * nouter), (unsigned)threads, smem, st, a, ntx);
 }
 
 // Threads per line for a length (host side).

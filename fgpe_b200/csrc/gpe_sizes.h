@@ -5,8 +5,8 @@
 #ifdef GPE_DEV_SIZES
 #define GPE_SIZES_p2(X) X(1) X(4) X(8) X(16) X(32) X(64) X(128)
 #define GPE_SIZES_p3(X) X(6) X(12) X(24) X(96)
-#define GPE_SIZES_p5(X) X(5) X(10) X(20) X(25)
-#define GPE_SIZES_p9(X) X(9)
+#define GPE_SIZES_p5(X) X(5) X(10) X(20) X(40) X(25)
+#define GPE_SIZES_p9(X) X(9) X(27)
 #else
 #define GPE_SIZES_p2(X) X(1) X(2) X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
 #define GPE_SIZES_p3(X) X(3) X(6) X(12) X(24) X(48) X(96) X(192) X(384) X(768)

@@ -96,6 +96,37 @@ def test_real_time_rk4(gpu, prec, shape):
 
 
 @pytest.mark.parametrize("prec", [C128, C64])
+@pytest.mark.parametrize("shape", [(16, 16, 16), (32, 24, 1)])
+def test_real_time_call_splitting(gpu, prec, shape):
+    # The x-inverse epilogue of each stage also transforms the next stage's
+    # input; a later call reuses that transform unless something else ran in
+    # between.  One call of 6 steps, 6 calls of 1 step, and calls with other
+    # operations (set_psi of the same state, observables) in between must
+    # give the same bits.
+    prms = np.zeros(32)
+    prms[:6] = [30.0 / (4 * PI_REF), 33.0 / (4 * PI_REF), 36.0 / (4 * PI_REF), 0.0, 0.003, 0.006]
+    cfg = make_config(shape, (5.0, 4.0, 3.0), dt=1e-3, precision=prec, prms=prms)
+    g1, o = pair(cfg)
+    g2, _ = pair(cfg)
+    g3, _ = pair(cfg)
+    g1.step_real(0, 6)
+    for k in range(6):
+        g2.step_real(k, 1)
+    for k in range(6):
+        g3.step_real(k, 1)
+        if k == 2:
+            g3.set_psi(0, g3.get_psi(0))
+        if k == 4:
+            g3.observables(0.0)
+    o.step_real(0, 6)
+    p1 = g1.get_psi(0)
+    assert np.array_equal(p1, g2.get_psi(0))
+    assert np.array_equal(p1, g3.get_psi(0))
+    tol = TOL[prec] if prec == C128 else 1e-5
+    assert rel(p1, o.get_psi(0)) < tol
+
+
+@pytest.mark.parametrize("prec", [C128, C64])
 @pytest.mark.parametrize("shape", [(16, 16, 16), (12, 10, 8), (32, 24, 1), (64, 1, 1)])
 def test_imag_heavyball(gpu, prec, shape):
     cfg = make_config(shape, (5.0, 4.0, 3.0), dt=2e-3, precision=prec, g=25.0, beta=0.9, epsilon_e=0.0)
