@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--quick", action="store_true", help="skip the 10^4-step accuracy run and the CPU baseline")
     p.add_argument("--grid", type=int, default=N_GRID)
     p.add_argument("--ground-steps", type=int, default=3000, help="heavy-ball iterations for the initial state")
+    p.add_argument("--cufft", action="store_true",
+                   help="print the comparison line: cuFFT (torch.fft) 3D forward + inverse at the same grid")
     return p.parse_args()
 
 
@@ -414,8 +416,36 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def run_cufft(args):
+    """Comparison only: one 3D forward + inverse transform pair with cuFFT
+    (through torch.fft) per precision, L2 flushed before each pair."""
+    import torch
+    n = args.grid
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    out = {"impl": "cuFFT (torch.fft.fftn + ifftn), comparison only", "grid": [n, n, n]}
+    for name, dt in (("c64", torch.complex64), ("c128", torch.complex128)):
+        x = torch.randn(n, n, n, dtype=dt, device="cuda")
+        for _ in range(3):
+            torch.fft.ifftn(torch.fft.fftn(x))
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(20)]
+        for a, b in evs:
+            flush.zero_()
+            a.record()
+            y = torch.fft.fftn(x)
+            x = torch.fft.ifftn(y)
+            b.record()
+        torch.cuda.synchronize()
+        ms = sorted(a.elapsed_time(b) for a, b in evs)[len(evs) // 2]
+        out[name + "_fwd_inv_pair_ms"] = round(ms, 5)
+    print(json.dumps(out))
+
+
 def main():
     args = parse()
+    if args.cufft:
+        run_cufft(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

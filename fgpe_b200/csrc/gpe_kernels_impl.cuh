@@ -500,11 +500,12 @@ __host__ __device__ constexpr int pass_min_blocks() {
 // ---- X pass -----------------------------------------------------------------------
 // One CTA = `rows` consecutive rows of the x axis, T threads per row.  Shared
 // memory: one padded exchange row per line (rows * xpad(L) elements).
-// Roles with the FP64 reductions hold more live values: one CTA fewer.
+// Roles with the FP64 reductions, and the fused RK + forward role, hold more
+// live values: one CTA fewer where three were asked for.
 template <typename R, int L, int NF, int KIND>
 __host__ __device__ constexpr int xpass_min_blocks() {
-    return kind_reduces<KIND>() && pass_min_blocks<R, L, NF>() > 1 ? pass_min_blocks<R, L, NF>() - 1
-                                                                    : pass_min_blocks<R, L, NF>();
+    return (kind_reduces<KIND>() || KIND == XK_RKF) && pass_min_blocks<R, L, NF>() > 2 ? pass_min_blocks<R, L, NF>() - 1
+                                                                                       : pass_min_blocks<R, L, NF>();
 }
 
 template <typename R, int L, int NF, int KIND>
@@ -615,8 +616,15 @@ __global__ void __launch_bounds__(256, (xpass_min_blocks<R, L, NF, KIND>())) k_x
 // b of the tile, thread t of the line); b is the fast index so that a warp
 // loads tx consecutive x values per line position.  Shared memory: the
 // exchange buffer S[pos * tx + b].
+// Strided passes hold no epilogue state: one CTA more than pass_min_blocks
+// for the short (complex64, E <= 8) lines.
 template <typename R, int L, int NF>
-__global__ void __launch_bounds__(256, (pass_min_blocks<R, L, NF>())) k_spass(PassArgs<R> a, int ntx) {
+__host__ __device__ constexpr int spass_min_blocks() {
+    return pass_min_blocks<R, L, NF>() == 3 ? 4 : pass_min_blocks<R, L, NF>();
+}
+
+template <typename R, int L, int NF>
+__global__ void __launch_bounds__(256, (spass_min_blocks<R, L, NF>())) k_spass(PassArgs<R> a, int ntx) {
     typedef typename Cx<R>::T C;
     constexpr int E = Plan<L>::E;
     constexpr int T = Plan<L>::T;
