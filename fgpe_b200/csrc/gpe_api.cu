@@ -309,17 +309,14 @@ gpe_status launch_x(gpe_handle* h, PassArgs<R> a, int nf, int mode) {
 }
 
 // Strided pass along y (axis 1) or z (axis 2): tx consecutive x values per
-// CTA, 128-byte rows (16 complex64 / 8 complex128 values) when nx allows,
-// at most 256 threads.
+// CTA (spass_tx: 128-byte rows, 16 complex64 / 8 complex128 values, at most
+// 256 threads); x blocks past nx are masked.
 template <typename R>
 gpe_status launch_s(gpe_handle* h, PassArgs<R> a, int nf, int axis, int mode) {
     typedef typename Cx<R>::T C;
     ProfScope ps(h, prof_kind(mode));
     const int L = axis == 1 ? h->ny : h->nz;
-    const int T = plan_T(L);
-    int tx = (int)(128 / sizeof(C));
-    if (tx > h->nx) tx = h->nx;
-    while (tx > 1 && tx * T > 256) tx /= 2;
+    const int tx = spass_tx(L, (int)sizeof(C));
     a.mode = mode;
     a.sax = axis;
     a.tx = tx;

@@ -59,7 +59,7 @@ struct PassArgs {
     int nrows;               // X pass: rows = ny*nz
     int ncomp;               // 1 or 2
     int dens;                // 1: field index ncomp is the dipolar density
-    int tx;                  // strided pass: lines (x values) per CTA
+    int tx;                  // strided pass: lines (x values) per CTA, spass_tx(L, sizeof(C))
     int mode, pro, epi, spec, stage, ham, sax;
     int check_done;          // exit when sc->done is set (stepping chunks)
     int want_obs;            // RK stage 4: logging reductions
@@ -86,6 +86,17 @@ struct PassArgs {
     double c_re, c_im;       // RK stage coefficient (stage 1..3 axpy; final uses c/6)
 };
 
+// Strided pass tile width: x values per CTA, the largest power of two up to
+// 128 bytes of a row (16 complex64 / 8 complex128 values) whose CTA of
+// tx * T threads stays within 256 threads.  A compile-time constant of the
+// kernel, so that the shared-memory column addressing folds into offsets.
+__host__ __device__ constexpr int spass_tx(int L, int esz) {
+    const int T = L / make_plan(L).E;
+    int tx = 128 / esz;
+    while (tx > 1 && tx * T > 256) tx /= 2;
+    return tx;
+}
+
 // ---- shared-memory line addressing -----------------------------------------
 // X pass exchange rows are padded by one slot every 8 elements: the first
 // radix-8 Stockham pass stores with stride 8, which would put the 16 lanes of
@@ -95,10 +106,9 @@ template <typename C> struct RowAddr {      // X pass: S[b*xpad(L) + pos + pos/8
     C* base;
     __device__ __forceinline__ C* operator()(unsigned pos) const { return base + (pos + (pos >> 3)); }
 };
-template <typename C> struct ColAddr {      // strided pass: S[pos*tx + b]
+template <typename C, int TX> struct ColAddr {  // strided pass: S[pos*TX + b]
     C* base;
-    unsigned tx;
-    __device__ __forceinline__ C* operator()(unsigned pos) const { return base + pos * tx; }
+    __device__ __forceinline__ C* operator()(unsigned pos) const { return base + pos * (unsigned)TX; }
 };
 
 // ---- compensated FP64 reductions --------------------------------------------

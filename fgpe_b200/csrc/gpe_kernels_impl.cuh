@@ -500,12 +500,11 @@ __host__ __device__ constexpr int pass_min_blocks() {
 // ---- X pass -----------------------------------------------------------------------
 // One CTA = `rows` consecutive rows of the x axis, T threads per row.  Shared
 // memory: one padded exchange row per line (rows * xpad(L) elements).
-// Roles with the FP64 reductions, and the fused RK + forward role, hold more
-// live values: one CTA fewer where three were asked for.
+// Roles with the FP64 reductions hold more live values: one CTA fewer.
 template <typename R, int L, int NF, int KIND>
 __host__ __device__ constexpr int xpass_min_blocks() {
-    return (kind_reduces<KIND>() || KIND == XK_RKF) && pass_min_blocks<R, L, NF>() > 2 ? pass_min_blocks<R, L, NF>() - 1
-                                                                                       : pass_min_blocks<R, L, NF>();
+    return kind_reduces<KIND>() && pass_min_blocks<R, L, NF>() > 1 ? pass_min_blocks<R, L, NF>() - 1
+                                                                    : pass_min_blocks<R, L, NF>();
 }
 
 template <typename R, int L, int NF, int KIND>
@@ -635,7 +634,7 @@ __global__ void __launch_bounds__(256, (spass_min_blocks<R, L, NF>())) k_spass(P
     if (a.check_done && a.sc->done) return;
 
     C* X = reinterpret_cast<C*>(smem_raw);
-    const int tx = a.tx;
+    constexpr int tx = spass_tx(L, (int)sizeof(C));
     const int xb = blockIdx.x % ntx, outer = blockIdx.x / ntx;
     const int x0 = xb * tx;
     const unsigned b = threadIdx.x % tx, t = threadIdx.x / tx;
@@ -643,7 +642,7 @@ __global__ void __launch_bounds__(256, (spass_min_blocks<R, L, NF>())) k_spass(P
     const long long ss = a.sstride;
     // g0 + reg_off(e) * ss: global index of register e of this thread's line
     const long long g0 = (long long)outer * a.ostride + x0 + (valid ? b : 0) + (long long)t * ss;
-    const ColAddr<C> addr{X + b, (unsigned)tx};
+    const ColAddr<C, tx> addr{X + b};
     const int mode = a.mode;
     C v[NF][E];
 
@@ -780,8 +779,9 @@ cudaError_t launch_spass(const PassArgs<R>& a, int nouter, size_t smem, cudaStre
     static bool attr = false;
     cudaError_t e = allow_smem(k_spass<R, L, NF>, smem, attr);
     if (e != cudaSuccess) return e;
-    const int threads = a.tx * Plan<L>::T;
-    const int ntx = (a.nx + a.tx - 1) / a.tx;
+    constexpr int tx = spass_tx(L, (int)sizeof(typename Cx<R>::T));
+    const int threads = tx * Plan<L>::T;
+    const int ntx = (a.nx + tx - 1) / tx;
     return launch_pass(k_spass<R, L, NF>, (unsigned)(ntx * nouter), (unsigned)threads, smem, st, a, ntx);
 }
 
