@@ -99,6 +99,15 @@ def lib() -> ctypes.CDLL:
         "gpe_kernel_launches": (c_longlong, [H]),
         "gpe_profile_enable": (c_int, [H, c_int]),
         "gpe_profile_read": (c_int, [H, P, POINTER(c_longlong)]),
+        "gpe_batch_create": (c_int, [POINTER(GPEConfig), c_int, POINTER(H)]),
+        "gpe_batch_destroy": (c_int, [H]),
+        "gpe_batch_set_stream": (c_int, [H, c_void_p]),
+        "gpe_batch_set_psi": (c_int, [H, c_int, P]),
+        "gpe_batch_set_vext": (c_int, [H, c_int, P]),
+        "gpe_batch_get_psi": (c_int, [H, c_int, P]),
+        "gpe_batch_step_imag": (c_int, [H, c_int, POINTER(c_int), POINTER(c_int)]),
+        "gpe_batch_imag_state": (c_int, [H, c_int, P]),
+        "gpe_batch_kernel_launches": (c_longlong, [H]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -289,3 +298,74 @@ class Solver:
         cnt = (c_longlong * len(self.PROF_KINDS))()
         _check(lib().gpe_profile_read(self._h, _dp(ms), cnt))
         return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.PROF_KINDS)}
+
+
+class Batch:
+    """Independent one-component instances advanced together (gpe_batch):
+    instances of equal geometry share every pass launch, one iteration of
+    all groups is a CUDA graph on a non-default stream."""
+
+    def __init__(self, cfgs):
+        self.cfgs = [c.copy() for c in cfgs]
+        arr = (GPEConfig * len(cfgs))(*self.cfgs)
+        h = c_void_p()
+        _check(lib().gpe_batch_create(arr, len(cfgs), byref(h)))
+        self._h = h
+        self.n = len(cfgs)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gpe_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _c128(self, i, arr):
+        c = self.cfgs[i]
+        a = np.ascontiguousarray(arr, dtype=np.complex128).reshape(-1)
+        if a.size != c.nx * c.ny * c.nz:
+            raise ValueError(f"instance {i}: expected {c.nx * c.ny * c.nz} points, got {a.size}")
+        return a
+
+    def set_stream(self, stream_ptr: int) -> None:
+        _check(lib().gpe_batch_set_stream(self._h, c_void_p(stream_ptr)))
+
+    def set_psi(self, i: int, psi) -> None:
+        a = self._c128(i, psi)
+        _check(lib().gpe_batch_set_psi(self._h, i, _dp(a.view(np.float64))))
+
+    def set_vext(self, i: int, v) -> None:
+        a = self._c128(i, v)
+        _check(lib().gpe_batch_set_vext(self._h, i, _dp(a.view(np.float64))))
+
+    def get_psi(self, i: int) -> np.ndarray:
+        c = self.cfgs[i]
+        out = np.empty(c.nx * c.ny * c.nz, np.complex128)
+        _check(lib().gpe_batch_get_psi(self._h, i, _dp(out.view(np.float64))))
+        return out.reshape(c.nz, c.ny, c.nx)
+
+    def step_imag(self, nsteps: int):
+        """Returns (iterations done per instance, converged flag per instance)."""
+        it = (c_int * self.n)()
+        cv = (c_int * self.n)()
+        _check(lib().gpe_batch_step_imag(self._h, nsteps, it, cv))
+        return np.array(it[:], dtype=np.int64), np.array(cv[:], dtype=bool)
+
+    def imag_state(self, i: int) -> np.ndarray:
+        out = np.zeros(4)
+        _check(lib().gpe_batch_imag_state(self._h, i, _dp(out)))
+        return out
+
+    @property
+    def launches(self) -> int:
+        return int(lib().gpe_batch_kernel_launches(self._h))

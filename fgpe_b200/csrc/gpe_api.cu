@@ -62,6 +62,7 @@ struct gpe_handle {
     int nx = 1, ny = 1, nz = 1;
     long long N = 1;
     int ncomp = 1, dens = 0, nf = 1;
+    int nb = 1;  // instances held (gpe_batch groups); fields of instance i start at i*N
     size_t esz = 16;
     cudaStream_t st = 0;
     void* A[2] = {nullptr, nullptr};
@@ -130,6 +131,10 @@ __global__ void k_canon(C* A, C* B, const DevScalars* sc, int comp, int hb, long
         const C a = A[i];
         A[i] = from_d<C>(make_double2((double)a.x * sc0, (double)a.y * sc0));
     }
+}
+__global__ void k_reset_iters(DevScalars* sc, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) sc[i].iters_done = 0;
 }
 __global__ void k_reset_scales(DevScalars* sc) {
     sc->scale[0][0] = sc->scale[0][1] = sc->scale[1][0] = sc->scale[1][1] = 1.0;
@@ -243,6 +248,9 @@ PassArgs<R> base_args(gpe_handle* h) {
     a.eps = h->cfg.epsilon_e;
     a.npart[0] = h->cfg.npart[0];
     a.npart[1] = h->cfg.npart[1];
+    a.nbatch = h->nb;
+    a.bstride = h->nb > 1 ? h->N : 0;
+    a.pstride = (long long)h->ny * h->nz * MAXQ * 2;
     return a;
 }
 
@@ -379,13 +387,15 @@ gpe_status canonicalize_t(gpe_handle* h) {
     if (h->mode == ST_CANON) return GPE_OK;
     h->w_fwd_A = false;
     const int thr = 256;
-    for (int c = 0; c < h->ncomp; ++c) {
-        k_canon<C><<<blocks_for(h->N, thr), thr, 0, h->st>>>((C*)h->A[c], (C*)h->B[c], h->sc, c, h->mode == ST_HB,
-                                                             h->N);
+    for (int i = 0; i < h->nb; ++i) {
+        for (int c = 0; c < h->ncomp; ++c) {
+            k_canon<C><<<blocks_for(h->N, thr), thr, 0, h->st>>>((C*)h->A[c] + i * h->N, (C*)h->B[c] + i * h->N,
+                                                                 h->sc + i, c, h->mode == ST_HB, h->N);
+            h->launches++;
+        }
+        k_reset_scales<<<1, 1, 0, h->st>>>(h->sc + i);
         h->launches++;
     }
-    k_reset_scales<<<1, 1, 0, h->st>>>(h->sc);
-    h->launches++;
     GPE_CUDA(cudaGetLastError());
     if (h->mode == ST_RKI) h->hb_old_valid = false;
     h->mode = ST_CANON;
@@ -399,7 +409,7 @@ gpe_status canonicalize(gpe_handle* h) {
 template <typename R>
 gpe_status copy_field(gpe_handle* h, void* dst, const void* src) {
     typedef typename Cx<R>::T C;
-    k_copy<C><<<blocks_for(h->N, 256), 256, 0, h->st>>>((C*)dst, (const C*)src, h->N);
+    k_copy<C><<<blocks_for(h->N * h->nb, 256), 256, 0, h->st>>>((C*)dst, (const C*)src, h->N * h->nb);
     h->launches++;
     GPE_CUDA(cudaGetLastError());
     return GPE_OK;
@@ -446,11 +456,11 @@ gpe_status step_real_t(gpe_handle* h, int first, int nsteps, double* obs_out) {
     return GPE_OK;
 }
 
+// State-mode switch before imaginary-time iterations: RK4 keeps psi in A with
+// a lazy scale; heavy ball needs psi_old in B.
 template <typename R>
-gpe_status step_imag_t(gpe_handle* h, int first, int nsteps, int* iters_done, int* converged) {
+gpe_status imag_prepare(gpe_handle* h) {
     h->w_fwd_A = false;
-    typedef typename Cx<R>::T C;
-    const double dt = h->cfg.dt;
     const bool rk = h->cfg.imag_scheme == GPE_IMAG_RK4;
     if (rk) {
         if (h->mode == ST_HB) GPE_TRY(canonicalize_t<R>(h));
@@ -464,9 +474,19 @@ gpe_status step_imag_t(gpe_handle* h, int first, int nsteps, int* iters_done, in
         }
         h->mode = ST_HB;
     }
-    // Reset the per-call iteration counter.
-    static const int zero = 0;
-    GPE_CUDA(cudaMemcpyAsync(&h->sc->iters_done, &zero, sizeof(int), cudaMemcpyHostToDevice, h->st));
+    // Reset the per-call iteration counters.
+    k_reset_iters<<<blocks_for(h->nb, 128), 128, 0, h->st>>>(h->sc, h->nb);
+    h->launches++;
+    GPE_CUDA(cudaGetLastError());
+    return GPE_OK;
+}
+
+// Launches nsteps imaginary-time iterations (no synchronisation).
+template <typename R>
+gpe_status imag_issue(gpe_handle* h, int first, int nsteps) {
+    typedef typename Cx<R>::T C;
+    const double dt = h->cfg.dt;
+    const bool rk = h->cfg.imag_scheme == GPE_IMAG_RK4;
     PassArgs<R> a = base_args<R>(h);
     a.check_done = 1;
     for (int j = 0; j < nsteps; ++j) {
@@ -489,6 +509,13 @@ gpe_status step_imag_t(gpe_handle* h, int first, int nsteps, int* iters_done, in
             }
         }
     }
+    return GPE_OK;
+}
+
+template <typename R>
+gpe_status step_imag_t(gpe_handle* h, int first, int nsteps, int* iters_done, int* converged) {
+    GPE_TRY(imag_prepare<R>(h));
+    GPE_TRY(imag_issue<R>(h, first, nsteps));
     DevScalars s;
     GPE_TRY(sync_read_scalars(h, &s));
     if (iters_done) *iters_done = s.iters_done;
@@ -651,7 +678,14 @@ gpe_status gpe_config_init(gpe_config* cfg) {
 
 int gpe_fft_length_supported(int n) { return (n >= 1 && make_plan(n).ok && length_compiled(n)) ? 1 : 0; }
 
-gpe_status gpe_create(const gpe_config* cfg, gpe_handle** out) {
+}  // extern "C"
+
+namespace {
+
+// A handle holding nb instances of one configuration (nb > 1: a gpe_batch
+// group; instance i's fields start at element i*N, its parameters, scalars
+// and partial sums at prms + 32*i, sc + i, partials + ny*nz*MAXQ*2*i).
+gpe_status create_handle(const gpe_config* cfg, int nb, gpe_handle** out) {
     if (!cfg || !out) return fail(GPE_ERR_INVALID_ARG, "null argument");
     *out = nullptr;
     if (cfg->abi_version != GPE_ABI_VERSION) return fail(GPE_ERR_INVALID_ARG, "abi_version mismatch");
@@ -684,6 +718,7 @@ gpe_status gpe_create(const gpe_config* cfg, gpe_handle** out) {
     h->dens = cfg->hamiltonian == GPE_HAM_DIPOLAR ? 1 : 0;
     h->nf = h->ncomp + h->dens;
     h->esz = h->prec == GPE_C128 ? 16 : 8;
+    h->nb = nb;
 
     auto bail = [&](gpe_status s) {
         free_all(h);
@@ -698,7 +733,7 @@ gpe_status gpe_create(const gpe_config* cfg, gpe_handle** out) {
         }
         return true;
     };
-    const size_t fb = h->esz * h->N;
+    const size_t fb = h->esz * h->N * nb;
     for (int c = 0; c < h->ncomp; ++c) {
         if (!dmalloc(&h->A[c], fb) || !dmalloc(&h->B[c], fb) || !dmalloc(&h->K[c], fb) || !dmalloc(&h->V[c], fb))
             return bail(GPE_ERR_OUT_OF_MEMORY);
@@ -741,19 +776,23 @@ gpe_status gpe_create(const gpe_config* cfg, gpe_handle** out) {
             cudaMemcpy(h->vdd, vf.data(), sizeof(float) * h->N, cudaMemcpyHostToDevice);
         }
     }
-    if (!dmalloc((void**)&h->prms, sizeof(double) * GPE_NO_HAMIL_PARAMS)) return bail(GPE_ERR_OUT_OF_MEMORY);
-    cudaMemcpy(h->prms, cfg->prms, sizeof(double) * GPE_NO_HAMIL_PARAMS, cudaMemcpyHostToDevice);
-    if (!dmalloc((void**)&h->sc, sizeof(DevScalars))) return bail(GPE_ERR_OUT_OF_MEMORY);
+    if (!dmalloc((void**)&h->prms, sizeof(double) * GPE_NO_HAMIL_PARAMS * nb)) return bail(GPE_ERR_OUT_OF_MEMORY);
+    if (!dmalloc((void**)&h->sc, sizeof(DevScalars) * nb)) return bail(GPE_ERR_OUT_OF_MEMORY);
     {
         DevScalars s;
         std::memset(&s, 0, sizeof(s));
         s.scale[0][0] = s.scale[0][1] = s.scale[1][0] = s.scale[1][1] = 1.0;
         s.norm[0] = cfg->npart[0];
         s.norm[1] = cfg->npart[1];
-        cudaMemcpy(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice);
+        std::vector<DevScalars> sv(nb, s);
+        std::vector<double> pv((size_t)GPE_NO_HAMIL_PARAMS * nb);
+        for (int i = 0; i < nb; ++i)
+            std::memcpy(pv.data() + (size_t)i * GPE_NO_HAMIL_PARAMS, cfg->prms, sizeof(double) * GPE_NO_HAMIL_PARAMS);
+        cudaMemcpy(h->sc, sv.data(), sizeof(DevScalars) * nb, cudaMemcpyHostToDevice);
+        cudaMemcpy(h->prms, pv.data(), sizeof(double) * pv.size(), cudaMemcpyHostToDevice);
     }
     const size_t nblk = (size_t)h->ny * h->nz;  // x-pass CTAs hold >= 1 row each
-    if (!dmalloc((void**)&h->partials, nblk * MAXQ * 2 * sizeof(double))) return bail(GPE_ERR_OUT_OF_MEMORY);
+    if (!dmalloc((void**)&h->partials, nblk * MAXQ * 2 * sizeof(double) * nb)) return bail(GPE_ERR_OUT_OF_MEMORY);
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         g_err = std::string("gpe_create: ") + cudaGetErrorString(e);
@@ -762,6 +801,12 @@ gpe_status gpe_create(const gpe_config* cfg, gpe_handle** out) {
     *out = h;
     return GPE_OK;
 }
+
+}  // namespace
+
+extern "C" {
+
+gpe_status gpe_create(const gpe_config* cfg, gpe_handle** out) { return create_handle(cfg, 1, out); }
 
 gpe_status gpe_destroy(gpe_handle* h) {
     if (!h) return GPE_OK;
@@ -983,6 +1028,263 @@ gpe_status gpe_profile_read(gpe_handle* h, double* ms_out, long long* count_out)
         if (count_out) count_out[k] = cnt[k];
     }
     return GPE_OK;
+}
+
+// ---- batched independent instances -------------------------------------------------------
+}  // extern "C"
+
+struct gpe_batch {
+    int n = 0;
+    int prec = GPE_C128;
+    std::vector<gpe_handle*> groups;     // one per distinct grid geometry
+    std::vector<int> gidx, ginst;        // instance -> group, index within the group
+    cudaStream_t st = 0;
+    cudaGraphExec_t exec = nullptr;      // one iteration of every group
+    cudaGraph_t graph = nullptr;
+    bool use_graph = true;
+    long long graph_launches = 0;        // kernels per replay of the graph
+    long long replayed = 0;              // kernels run by graph replays
+};
+
+namespace {
+
+bool same_geometry(const gpe_config& a, const gpe_config& b) {
+    if (a.nx != b.nx || a.ny != b.ny || a.nz != b.nz || a.dim != b.dim) return false;
+    for (int d = 0; d < 3; ++d)
+        if (a.xmax[d] != b.xmax[d] || a.dx[d] != b.dx[d]) return false;
+    return true;
+}
+
+gpe_status batch_inst(gpe_batch* b, int inst, gpe_handle** h, size_t* off) {
+    if (!b) return fail(GPE_ERR_INVALID_ARG, "null batch");
+    if (inst < 0 || inst >= b->n) return fail(GPE_ERR_INVALID_ARG, "instance index out of range");
+    *h = b->groups[b->gidx[inst]];
+    *off = (size_t)b->ginst[inst] * (size_t)(*h)->N * (*h)->esz;
+    return GPE_OK;
+}
+
+void batch_drop_graph(gpe_batch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+
+template <typename R>
+gpe_status batch_issue_iteration(gpe_batch* b) {
+    for (gpe_handle* h : b->groups) GPE_TRY(imag_issue<R>(h, 0, 1));
+    return GPE_OK;
+}
+
+// Captures one imaginary-time iteration of every group into a CUDA graph.
+template <typename R>
+gpe_status batch_capture(gpe_batch* b) {
+    if (b->exec || !b->use_graph) return GPE_OK;
+    if (b->st == 0) {
+        b->use_graph = false;  // the legacy default stream cannot be captured
+        return GPE_OK;
+    }
+    long long before = 0, after = 0;
+    for (gpe_handle* h : b->groups) before += h->launches;
+    GPE_CUDA(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+    gpe_status s = batch_issue_iteration<R>(b);
+    for (gpe_handle* h : b->groups) after += h->launches;
+    // captured launches have not run: count them per replay instead
+    b->graph_launches = after - before;
+    b->replayed -= after - before;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b->st, &g);
+    if (s != GPE_OK || e != cudaSuccess || !g) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        b->replayed += b->graph_launches;
+        b->graph_launches = 0;
+        b->use_graph = false;  // fall back to direct launches
+        return GPE_OK;
+    }
+    b->graph = g;
+    e = cudaGraphInstantiate(&b->exec, g, 0);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        batch_drop_graph(b);
+        b->replayed += b->graph_launches;
+        b->graph_launches = 0;
+        b->use_graph = false;
+    }
+    return GPE_OK;
+}
+
+template <typename R>
+gpe_status batch_step_imag_t(gpe_batch* b, int nsteps, int* iters_done, int* converged) {
+    for (gpe_handle* h : b->groups) GPE_TRY(imag_prepare<R>(h));
+    GPE_TRY(batch_capture<R>(b));
+    for (int j = 0; j < nsteps; ++j) {
+        if (b->exec) {
+            GPE_CUDA(cudaGraphLaunch(b->exec, b->st));
+            b->replayed += b->graph_launches;
+        } else {
+            GPE_TRY(batch_issue_iteration<R>(b));
+        }
+    }
+    GPE_CUDA(cudaStreamSynchronize(b->st));
+    GPE_CUDA(cudaGetLastError());
+    bool diverged = false;
+    std::vector<DevScalars> sv;
+    for (size_t g = 0; g < b->groups.size(); ++g) {
+        gpe_handle* h = b->groups[g];
+        sv.resize(h->nb);
+        GPE_CUDA(cudaMemcpy(sv.data(), h->sc, sizeof(DevScalars) * h->nb, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < b->n; ++i) {
+            if (b->gidx[i] != (int)g) continue;
+            const DevScalars& d = sv[b->ginst[i]];
+            if (iters_done) iters_done[i] = d.iters_done;
+            if (converged) converged[i] = d.converged;
+            diverged = diverged || d.status == GPE_ERR_DIVERGED;
+        }
+    }
+    if (diverged) return fail(GPE_ERR_DIVERGED, "an instance has a non-finite norm, energy or chemical potential");
+    return GPE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gpe_status gpe_batch_create(const gpe_config* cfgs, int n, gpe_batch** out) {
+    if (!cfgs || !out || n < 1) return fail(GPE_ERR_INVALID_ARG, "null argument or n < 1");
+    *out = nullptr;
+    const gpe_config& c0 = cfgs[0];
+    for (int i = 0; i < n; ++i) {
+        const gpe_config& c = cfgs[i];
+        if (c.abi_version != GPE_ABI_VERSION) return fail(GPE_ERR_INVALID_ARG, "abi_version mismatch");
+        if (c.ncomp != 1) return fail(GPE_ERR_UNSUPPORTED, "batched instances have one component");
+        if (c.hamiltonian != GPE_HAM_BEC && c.hamiltonian != GPE_HAM_TEMPLATE)
+            return fail(GPE_ERR_UNSUPPORTED, "batched instances use GPE_HAM_BEC or GPE_HAM_TEMPLATE");
+        if (c.precision != c0.precision || c.hamiltonian != c0.hamiltonian || c.imag_scheme != c0.imag_scheme ||
+            c.dt != c0.dt || c.beta != c0.beta || c.epsilon_e != c0.epsilon_e || c.npart[0] != c0.npart[0])
+            return fail(GPE_ERR_INVALID_ARG,
+                        "batched instances share precision, hamiltonian, imag_scheme, dt, beta, epsilon_e, npart");
+        if (c.prms[3] > 0 || c.prms[4] > 0 || c.prms[5] > 0)
+            return fail(GPE_ERR_UNSUPPORTED, "batched instances have a time-independent coupling (prms[3..5] <= 0)");
+    }
+    gpe_batch* b = new gpe_batch();
+    b->n = n;
+    b->prec = c0.precision;
+    b->gidx.assign(n, -1);
+    b->ginst.assign(n, 0);
+    std::vector<std::vector<int>> members;
+    for (int i = 0; i < n; ++i) {
+        int g = -1;
+        for (size_t k = 0; k < members.size(); ++k)
+            if (same_geometry(cfgs[members[k][0]], cfgs[i])) g = (int)k;
+        if (g < 0) {
+            g = (int)members.size();
+            members.emplace_back();
+        }
+        b->gidx[i] = g;
+        b->ginst[i] = (int)members[g].size();
+        members[g].push_back(i);
+    }
+    for (auto& m : members) {
+        gpe_handle* h = nullptr;
+        gpe_status s = create_handle(&cfgs[m[0]], (int)m.size(), &h);
+        if (s != GPE_OK) {
+            gpe_batch_destroy(b);
+            return s;
+        }
+        b->groups.push_back(h);
+        for (size_t k = 0; k < m.size(); ++k)
+            cudaMemcpy(h->prms + k * GPE_NO_HAMIL_PARAMS, cfgs[m[k]].prms, sizeof(double) * GPE_NO_HAMIL_PARAMS,
+                       cudaMemcpyHostToDevice);
+    }
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        gpe_batch_destroy(b);
+        return fail(GPE_ERR_CUDA, std::string("gpe_batch_create: ") + cudaGetErrorString(e));
+    }
+    *out = b;
+    return GPE_OK;
+}
+
+gpe_status gpe_batch_destroy(gpe_batch* b) {
+    if (!b) return GPE_OK;
+    cudaStreamSynchronize(b->st);
+    batch_drop_graph(b);
+    for (gpe_handle* h : b->groups) {
+        free_all(h);
+        delete h;
+    }
+    delete b;
+    return GPE_OK;
+}
+
+gpe_status gpe_batch_set_stream(gpe_batch* b, void* cuda_stream) {
+    if (!b) return fail(GPE_ERR_INVALID_ARG, "null batch");
+    if ((cudaStream_t)cuda_stream != b->st) batch_drop_graph(b);
+    b->st = (cudaStream_t)cuda_stream;
+    b->use_graph = true;
+    for (gpe_handle* h : b->groups) h->st = b->st;
+    return GPE_OK;
+}
+
+gpe_status gpe_batch_set_psi(gpe_batch* b, int inst, const double* host_c128) {
+    gpe_handle* h;
+    size_t off;
+    GPE_TRY(batch_inst(b, inst, &h, &off));
+    if (!host_c128) return fail(GPE_ERR_INVALID_ARG, "null psi");
+    GPE_TRY(canonicalize(h));
+    char* A = (char*)h->A[0] + off;
+    GPE_TRY(upload_c128_host(h, host_c128, A));
+    GPE_CUDA(cudaMemcpyAsync((char*)h->B[0] + off, A, h->esz * h->N, cudaMemcpyDeviceToDevice, h->st));
+    GPE_CUDA(cudaStreamSynchronize(h->st));
+    h->hb_old_valid = true;
+    return GPE_OK;
+}
+
+gpe_status gpe_batch_set_vext(gpe_batch* b, int inst, const double* host_c128) {
+    gpe_handle* h;
+    size_t off;
+    GPE_TRY(batch_inst(b, inst, &h, &off));
+    if (!host_c128) return fail(GPE_ERR_INVALID_ARG, "null vext");
+    return upload_c128_host(h, host_c128, (char*)h->V[0] + off);
+}
+
+gpe_status gpe_batch_get_psi(gpe_batch* b, int inst, double* host_c128) {
+    gpe_handle* h;
+    size_t off;
+    GPE_TRY(batch_inst(b, inst, &h, &off));
+    if (!host_c128) return fail(GPE_ERR_INVALID_ARG, "null output");
+    GPE_TRY(canonicalize(h));
+    return download_c128_host(h, (char*)h->A[0] + off, host_c128);
+}
+
+gpe_status gpe_batch_step_imag(gpe_batch* b, int nsteps, int* iters_done, int* converged) {
+    if (!b) return fail(GPE_ERR_INVALID_ARG, "null batch");
+    if (nsteps < 0) return fail(GPE_ERR_INVALID_ARG, "nsteps < 0");
+    return b->prec == GPE_C64 ? batch_step_imag_t<float>(b, nsteps, iters_done, converged)
+                              : batch_step_imag_t<double>(b, nsteps, iters_done, converged);
+}
+
+gpe_status gpe_batch_imag_state(gpe_batch* b, int inst, double* out) {
+    gpe_handle* h;
+    size_t off;
+    GPE_TRY(batch_inst(b, inst, &h, &off));
+    if (!out) return fail(GPE_ERR_INVALID_ARG, "null output");
+    DevScalars d;
+    GPE_CUDA(cudaStreamSynchronize(h->st));
+    GPE_CUDA(cudaMemcpy(&d, h->sc + b->ginst[inst], sizeof(d), cudaMemcpyDeviceToHost));
+    out[0] = d.norm[0];
+    out[1] = d.mu[0];
+    out[2] = d.en[0];
+    out[3] = d.en_prev[0];
+    return GPE_OK;
+}
+
+long long gpe_batch_kernel_launches(const gpe_batch* b) {
+    if (!b) return 0;
+    long long n = b->replayed;
+    for (const gpe_handle* h : b->groups) n += h->launches;
+    return n;
 }
 
 }  // extern "C"

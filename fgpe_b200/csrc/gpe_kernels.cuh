@@ -64,6 +64,12 @@ struct PassArgs {
     int check_done;          // exit when sc->done is set (stepping chunks)
     int want_obs;            // RK stage 4: logging reductions
     int fuse_fwd;            // RK epilogue: also x-forward transform the new state into w
+    // Batched instances (gpe_batch): blockIdx.y selects the instance; its
+    // fields sit bstride elements apart, its d_h_params, scalars and partial
+    // sums at prms + 32*inst, sc + inst, partials + pstride*inst.
+    int nbatch;              // 1 for a single handle
+    long long bstride;
+    long long pstride;
     C* w[3];                 // transformed fields (work buffers)
     C* buf[2][2];            // [slot][comp] state buffers (A = slot 0, B = slot 1)
     C* kacc[2];              // RK accumulators

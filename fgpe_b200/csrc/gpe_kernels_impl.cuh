@@ -24,6 +24,18 @@ __device__ __forceinline__ void pass_prologue_sync() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// Batched launch: point a's per-instance members at instance blockIdx.y and
+// return the element offset of its fields.
+template <typename R>
+__device__ __forceinline__ long long select_instance(PassArgs<R>& a) {
+    if (a.nbatch <= 1) return 0;
+    const int inst = blockIdx.y;
+    a.sc += inst;
+    a.prms += (size_t)inst * GPE_NO_HAMIL_PARAMS;
+    a.partials += (size_t)inst * a.pstride;
+    return (long long)inst * a.bstride;
+}
+
 // Lazy normalisation factors of the current / previous heavy-ball slot.
 template <typename R>
 struct PsiScale {
@@ -189,7 +201,7 @@ __device__ void reduce_and_finalize(const PassArgs<R>& a, DD (&acc)[NQ], DD* red
         }
         __threadfence();
         const unsigned int ticket = atomicAdd(&a.sc->counter, 1u);
-        is_last = (ticket == gridDim.x * gridDim.y - 1) ? 1 : 0;
+        is_last = (ticket == gridDim.x - 1) ? 1 : 0;
     }
     __syncthreads();
     if (is_last) {
@@ -197,7 +209,7 @@ __device__ void reduce_and_finalize(const PassArgs<R>& a, DD (&acc)[NQ], DD* red
         DD s[NQ];
 #pragma unroll
         for (int q = 0; q < NQ; ++q) s[q] = DD{0.0, 0.0};
-        const unsigned int nb = gridDim.x * gridDim.y;
+        const unsigned int nb = gridDim.x;
         for (unsigned int i = threadIdx.x; i < nb; i += blockDim.x) {
             const double* p = a.partials + (size_t)i * NQ * 2;
 #pragma unroll
@@ -516,6 +528,7 @@ __global__ void __launch_bounds__(256, (xpass_min_blocks<R, L, NF, KIND>())) k_x
     constexpr int RoutF = Plan<L>::out_radix(false);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     pass_prologue_sync();
+    const long long boff = select_instance(a);
     if (a.check_done && a.sc->done) return;
 
     C* X = reinterpret_cast<C*>(smem_raw);
@@ -523,7 +536,7 @@ __global__ void __launch_bounds__(256, (xpass_min_blocks<R, L, NF, KIND>())) k_x
     const int row = blockIdx.x * rows + (int)b;
     const bool valid = row < a.nrows;
     // g0 + reg_off(e): global index of register e of this thread's line
-    const long long g0 = (long long)(valid ? row : 0) * L + t;
+    const long long g0 = boff + (long long)(valid ? row : 0) * L + t;
     const RowAddr<C> addr{X + b * xpad(L)};
     const int cur = a.sc->cur_slot;
     const PsiScale<R> ps = load_scales<R>(a, cur);
@@ -631,6 +644,7 @@ __global__ void __launch_bounds__(256, (spass_min_blocks<R, L, NF>())) k_spass(P
     constexpr int RoutF = Plan<L>::out_radix(false);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     pass_prologue_sync();
+    const long long boff = select_instance(a);
     if (a.check_done && a.sc->done) return;
 
     C* X = reinterpret_cast<C*>(smem_raw);
@@ -641,7 +655,7 @@ __global__ void __launch_bounds__(256, (spass_min_blocks<R, L, NF>())) k_spass(P
     const bool valid = x0 + (int)b < a.nx;
     const long long ss = a.sstride;
     // g0 + reg_off(e) * ss: global index of register e of this thread's line
-    const long long g0 = (long long)outer * a.ostride + x0 + (valid ? b : 0) + (long long)t * ss;
+    const long long g0 = boff + (long long)outer * a.ostride + x0 + (valid ? b : 0) + (long long)t * ss;
     const ColAddr<C, tx> addr{X + b};
     const int mode = a.mode;
     C v[NF][E];
@@ -709,9 +723,10 @@ __global__ void __launch_bounds__(256, (spass_min_blocks<R, L, NF>())) k_spass(P
 // rows: rows per CTA (x pass); smem: exchange buffer bytes; both chosen by the host.
 // Launch with programmatic stream serialization (see pass_prologue_sync).
 template <typename K, typename... Args>
-cudaError_t launch_pass(K kernel, unsigned grid, unsigned threads, size_t smem, cudaStream_t st, Args... args) {
+cudaError_t launch_pass(K kernel, unsigned grid, unsigned nbatch, unsigned threads, size_t smem, cudaStream_t st,
+                        Args... args) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
+    cfg.gridDim = dim3(grid, nbatch);
     cfg.blockDim = dim3(threads);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
@@ -740,7 +755,8 @@ cudaError_t launch_xpass_kind(const PassArgs<R>& a, int rows, size_t smem, cudaS
     if (e != cudaSuccess) return e;
     const int threads = rows * Plan<L>::T;
     const int grid = (a.nrows + rows - 1) / rows;
-    return launch_pass(k_xpass<R, L, NF, KIND>, (unsigned)grid, (unsigned)threads, smem, st, a, rows);
+    return launch_pass(k_xpass<R, L, NF, KIND>, (unsigned)grid, (unsigned)a.nbatch, (unsigned)threads, smem, st, a,
+                       rows);
 }
 
 // Kernel role from the pass mode and epilogue op.
@@ -782,7 +798,8 @@ cudaError_t launch_spass(const PassArgs<R>& a, int nouter, size_t smem, cudaStre
     constexpr int tx = spass_tx(L, (int)sizeof(typename Cx<R>::T));
     const int threads = tx * Plan<L>::T;
     const int ntx = (a.nx + tx - 1) / tx;
-    return launch_pass(k_spass<R, L, NF>, (unsigned)(ntx * nouter), (unsigned)threads, smem, st, a, ntx);
+    return launch_pass(k_spass<R, L, NF>, (unsigned)(ntx * nouter), (unsigned)a.nbatch, (unsigned)threads, smem, st,
+                       a, ntx);
 }
 
 // Threads per line for a length (host side).

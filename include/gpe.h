@@ -53,9 +53,10 @@ typedef enum gpe_status {
 /* Storage / arithmetic form of the fields.
  *  GPE_C128: complex128 everywhere (the drop-in; cuFFT Z2Z in the reference,
  *            src/parallel.cu:97-102).
- *  GPE_C64 : complex64 fields and FFT butterflies; stage axpy coefficients,
- *            norm, energy, chemical potential, renormalisation and the
- *            convergence test stay FP64 (compensated sums). */
+ *  GPE_C64 : complex64 fields, FFT butterflies and real-time RK4 stage
+ *            updates in FP32; norm, energy, chemical potential, the
+ *            imaginary-time update, renormalisation and the convergence
+ *            test stay FP64 (compensated sums). */
 typedef enum gpe_precision { GPE_C128 = 0, GPE_C64 = 1 } gpe_precision;
 
 /* Which Hamiltonian plugin supplies the pointwise term.
@@ -184,6 +185,35 @@ gpe_status gpe_momentum_x(gpe_handle* h, int comp, double* px);
 /* Unnormalised 3D DFT of psi_comp in place, sign -1 (CUFFT_FORWARD) or +1
  * (CUFFT_INVERSE): the cufftExecZ2Z calls of src/baseHamiltonian.cu:89,95. */
 gpe_status gpe_fft(gpe_handle* h, int comp, int sign);
+
+/* ---- batched independent instances (no counterpart in the reference, whose
+ * parameter sweeps are separate ./gpe runs) ----------------------------------
+ * A batch holds n one-component instances that may differ in grid geometry
+ * (nx, ny, nz, xmax, dx) and in d_h_params (e.g. the coupling); precision,
+ * hamiltonian (GPE_HAM_BEC or GPE_HAM_TEMPLATE), imag_scheme, dt, beta,
+ * epsilon_e and npart are shared, and the coupling is time-independent
+ * (prms[3..5] <= 0).  Instances with the same geometry form a group whose
+ * fields are contiguous; every pass kernel of a group advances all its
+ * instances in one launch (blockIdx.y = instance), and one imaginary-time
+ * iteration of every group is captured once into a CUDA graph that each
+ * iteration replays (direct launches on the legacy default stream).
+ * Instances that have converged skip their work on the device. */
+typedef struct gpe_batch gpe_batch;
+gpe_status gpe_batch_create(const gpe_config* cfgs, int n, gpe_batch** out);
+gpe_status gpe_batch_destroy(gpe_batch* b);
+gpe_status gpe_batch_set_stream(gpe_batch* b, void* cuda_stream);
+gpe_status gpe_batch_set_psi(gpe_batch* b, int inst, const double* host_c128);
+gpe_status gpe_batch_set_vext(gpe_batch* b, int inst, const double* host_c128);
+gpe_status gpe_batch_get_psi(gpe_batch* b, int inst, double* host_c128);
+/* Up to nsteps imaginary-time iterations of every unconverged instance (the
+ * scheme of gpe_step_imag at time 0).  Per instance i: iters_done[i] counts the
+ * iterations applied in this call, converged[i] is 1 once its test fired
+ * (arrays of n; either may be NULL). */
+gpe_status gpe_batch_step_imag(gpe_batch* b, int nsteps, int* iters_done, int* converged);
+/* gpe_imag_state of one instance: out[0..3] = NORM, MU, EN, EN_PREV. */
+gpe_status gpe_batch_imag_state(gpe_batch* b, int inst, double* out);
+/* Kernels of this library run for the batch so far (graph replays included). */
+long long  gpe_batch_kernel_launches(const gpe_batch* b);
 
 /* ---- allocation-free norm (no counterpart in the reference) -------------
  * dev_out[0] = DV * sum |psi[i]|^2 over n complex128 points of a caller-owned
