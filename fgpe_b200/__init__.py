@@ -99,6 +99,8 @@ def lib() -> ctypes.CDLL:
         "gpe_kernel_launches": (c_longlong, [H]),
         "gpe_profile_enable": (c_int, [H, c_int]),
         "gpe_profile_read": (c_int, [H, P, POINTER(c_longlong)]),
+        "gpe_control_set_basis": (c_int, [H, c_int, P]),
+        "gpe_control_gradient": (c_int, [H, P, c_int, P, c_int, P, P]),
         "gpe_batch_create": (c_int, [POINTER(GPEConfig), c_int, POINTER(H)]),
         "gpe_batch_destroy": (c_int, [H]),
         "gpe_batch_set_stream": (c_int, [H, c_void_p]),
@@ -252,6 +254,29 @@ class Solver:
         done, conv = c_int(0), c_int(0)
         _check(lib().gpe_step_imag(self._h, first_iteration, nsteps, byref(done), byref(conv)))
         return done.value, bool(conv.value)
+
+    def control_set_basis(self, G) -> None:
+        """Control basis functions G_k (real, shape (nctrl, nz, ny, nx))."""
+        g = np.ascontiguousarray(G, dtype=np.float64).reshape(-1)
+        if g.size % self.N:
+            raise ValueError("basis size is not a multiple of the grid size")
+        _check(lib().gpe_control_set_basis(self._h, g.size // self.N, _dp(g)))
+        self._nctrl = g.size // self.N
+
+    def control_gradient(self, u, target, checkpoint_every: int = 50, want_grad: bool = True):
+        """Infidelity 1 - |<target|psi(T)>|^2 after u.shape[0] controlled RK4
+        steps from the current state, and its gradient with respect to u
+        (shape (nsteps, nctrl)) by the adjoint.  The state is left unchanged."""
+        un = np.ascontiguousarray(u, dtype=np.float64)
+        if un.ndim != 2 or un.shape[1] != getattr(self, "_nctrl", -1):
+            raise ValueError("u must have shape (nsteps, nctrl)")
+        t = self._c128(target)
+        loss = c_double()
+        grad = np.zeros_like(un) if want_grad else None
+        _check(lib().gpe_control_gradient(self._h, _dp(un), un.shape[0], _dp(t.view(np.float64)),
+                                          int(checkpoint_every), byref(loss),
+                                          _dp(grad) if want_grad else None))
+        return loss.value, grad
 
     def imag_state(self) -> np.ndarray:
         out = np.zeros(8)

@@ -84,6 +84,17 @@ struct gpe_handle {
     // W[0..nf-1] hold the x-forward transform of the state in A (left by the
     // last real-time stage); any other operation clears it.
     bool w_fwd_A = false;
+    // control gradient (gpe_control_*): basis G[k] (real, field precision),
+    // saved base potential, work fields, checkpoints
+    int nctrl = 0;
+    void* ctrlG = nullptr;
+    void* V0 = nullptr;
+    void* adj[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    void* qf = nullptr;
+    double* d_u = nullptr;
+    double* d_part = nullptr;
+    double* d_grad = nullptr;
+    std::vector<void*> cps;
     // per-pass event timing (gpe_profile_enable)
     bool prof = false;
     std::vector<cudaEvent_t> ev_free;
@@ -142,6 +153,66 @@ __global__ void k_reset_scales(DevScalars* sc) {
 }
 
 inline unsigned blocks_for(long long n, int thr) { return (unsigned)((n + thr - 1) / thr); }
+
+// ---- control-gradient helpers ------------------------------------------------------------
+// V = V0 + sum_k u[k] G_k (real part), the potential of one controlled step.
+template <typename C, typename R>
+__global__ void k_form_control_v(C* V, const C* V0, const R* G, const double* u, int nctrl, long long n) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    C v = V0[i];
+    double w = (double)v.x;
+    for (int k = 0; k < nctrl; ++k) w += u[k] * (double)G[(long long)k * n + i];
+    v.x = (decltype(v.x))w;
+    V[i] = v;
+}
+// dst = (cr + i ci) * src
+template <typename C>
+__global__ void k_cscale(C* dst, const C* src, double cr, double ci, long long n) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const C a = src[i];
+    dst[i] = from_d<C>(make_double2(cr * a.x - ci * a.y, cr * a.y + ci * a.x));
+}
+// Per-block FP64 partial sums, fixed order: mode 0: sum conj(a) b (2 values);
+// mode 1: sum_x G_k(x) q(x) for k < nq (q real, G real).
+constexpr int CTRL_BLOCKS = 128;
+template <typename C, typename R>
+__global__ void k_ctrl_partials(int mode, const C* a, const C* b, const R* q, const R* G, int nq, long long n,
+                                double* part) {
+    __shared__ double sh[256];
+    double acc[2 * 64];
+    const int nv = mode == 0 ? 2 : nq;
+    for (int k = 0; k < nv; ++k) acc[k] = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        if (mode == 0) {
+            const C x = a[i], y = b[i];
+            acc[0] += (double)x.x * y.x + (double)x.y * y.y;
+            acc[1] += (double)x.x * y.y - (double)x.y * y.x;
+        } else {
+            const double qq = (double)q[i];
+            for (int k = 0; k < nq; ++k) acc[k] += (double)G[(long long)k * n + i] * qq;
+        }
+    }
+    for (int k = 0; k < nv; ++k) {
+        sh[threadIdx.x] = acc[k];
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) part[(long long)blockIdx.x * nv + k] = sh[0];
+        __syncthreads();
+    }
+}
+// out[k] = sum over blocks of part[b][k], block order.
+__global__ void k_ctrl_final(const double* part, int nblocks, int nv, double* out) {
+    const int k = threadIdx.x;
+    if (k >= nv) return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += part[(long long)b * nv + k];
+    out[k] = s;
+}
 
 // Host copy of the dipolar kernel (see gpe_config docs / GPE_HAM_DIPOLAR),
 // the unused DipoleDipoleInteraction of src/parallel.cu:326-352 with a
@@ -631,6 +702,12 @@ void free_all(gpe_handle* h) {
                     h->kax[1], h->kax[2], h->vdd, h->prms, h->sc, h->partials, h->stage128};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    void* cptrs[] = {h->ctrlG, h->V0, h->adj[0], h->adj[1], h->adj[2], h->adj[3], h->adj[4], h->adj[5], h->adj[6],
+                     h->qf, h->d_u, h->d_part, h->d_grad};
+    for (void* p : cptrs)
+        if (p) cudaFree(p);
+    for (void* p : h->cps)
+        if (p) cudaFree(p);
     for (auto& r : h->recs) {
         cudaEventDestroy(r.a);
         cudaEventDestroy(r.b);
@@ -681,6 +758,179 @@ int gpe_fft_length_supported(int n) { return (n >= 1 && make_plan(n).ok && lengt
 }  // extern "C"
 
 namespace {
+
+// ---- control gradient (the adjoint of the controlled real-time RK4 step) -----------------
+// One controlled step n: V <- V0 + sum_k u[n,k] G_k, then the real-time RK4
+// step of gpe_step_real.
+template <typename R>
+gpe_status ctrl_form_v(gpe_handle* h, int n) {
+    typedef typename Cx<R>::T C;
+    k_form_control_v<C, R><<<blocks_for(h->N, 256), 256, 0, h->st>>>((C*)h->V[0], (const C*)h->V0,
+                                                                      (const R*)h->ctrlG, h->d_u + (size_t)n * h->nctrl,
+                                                                      h->nctrl, h->N);
+    h->launches++;
+    GPE_CUDA(cudaGetLastError());
+    return GPE_OK;
+}
+
+// Stage arguments of step n from psi_n = S: Pa, Pb, Pc (RK stages 1-3 with
+// their states written to separate fields).
+template <typename R>
+gpe_status ctrl_stage_args(gpe_handle* h, void* S, void* Pa, void* Pb, void* Pc, int n) {
+    typedef typename Cx<R>::T C;
+    const double dt = h->cfg.dt;
+    PassArgs<R> a = base_args<R>(h);
+    a.epi = EPI_RK;
+    a.pro = PRO_PIN;
+    a.buf[0][0] = (C*)S;
+    void* outs[3] = {Pa, Pb, Pc};
+    const bool can_fuse = h->ny > 1 || h->nz > 1;
+    bool w_ready = false;
+    for (int s = 1; s <= 3; ++s) {
+        a.stage = s;
+        a.pin[0] = (const C*)(s == 1 ? S : outs[s - 2]);
+        a.buf[1][0] = (C*)outs[s - 1];
+        a.c_re = 0.0;
+        a.c_im = (s <= 2) ? -0.5 * dt : -1.0 * dt;
+        a.t = (s == 1) ? (double)n * dt : (n + 0.5) * dt;
+        a.want_obs = 0;
+        a.fuse_fwd = (can_fuse && s < 3) ? 1 : 0;
+        GPE_TRY(run_chain<R>(h, a, 1, w_ready));
+        w_ready = a.fuse_fwd != 0;
+    }
+    h->w_fwd_A = false;
+    return GPE_OK;
+}
+
+// Reverse of step n: lambda (adj[0]) <- lambda_n, q (qf) <- gradient density.
+template <typename R>
+gpe_status ctrl_adjoint_step(gpe_handle* h, void* S, void* Pa, void* Pb, void* Pc, int n) {
+    typedef typename Cx<R>::T C;
+    const double dt = h->cfg.dt;
+    C* lam = (C*)h->adj[0];
+    C* acc = (C*)h->adj[1];
+    C* mu = (C*)h->adj[2];
+    k_cscale<C><<<blocks_for(h->N, 256), 256, 0, h->st>>>(mu, lam, dt / 6.0, 0.0, h->N);
+    h->launches++;
+    PassArgs<R> a = base_args<R>(h);
+    a.epi = EPI_ADJ;
+    a.pro = PRO_PIN;
+    a.pin[0] = mu;
+    a.buf[1][0] = mu;
+    a.kacc[0] = acc;
+    a.out[0] = lam;
+    a.out[1] = (C*)h->qf;
+    void* args[5] = {nullptr, S, Pa, Pb, Pc};  // psi_s of stage s
+    const double cl[5] = {0.0, 0.0, dt / 6.0, dt / 3.0, dt / 3.0};   // lambda coefficient of the next mu
+    const double cj[5] = {0.0, 0.0, 0.5 * dt, 0.5 * dt, dt};         // jt coefficient of the next mu
+    for (int s = 4; s >= 1; --s) {
+        a.stage = s;
+        a.buf[0][0] = (C*)args[s];
+        a.c_re = cl[s];
+        a.c_im = cj[s];
+        a.t = (s == 1) ? (double)n * dt : (s < 4) ? (n + 0.5) * dt : (double)(n + 1) * dt;
+        GPE_TRY(run_chain<R>(h, a, 1));
+    }
+    h->w_fwd_A = false;
+    GPE_CUDA(cudaGetLastError());
+    return GPE_OK;
+}
+
+// grad[n*nctrl + k] = sum_x G_k(x) q(x), FP64, on the device.
+template <typename R>
+gpe_status ctrl_reduce_grad(gpe_handle* h, int n) {
+    typedef typename Cx<R>::T C;
+    k_ctrl_partials<C, R><<<CTRL_BLOCKS, 256, 0, h->st>>>(1, nullptr, nullptr, (const R*)h->qf, (const R*)h->ctrlG,
+                                                         h->nctrl, h->N, h->d_part);
+    k_ctrl_final<<<1, 64, 0, h->st>>>(h->d_part, CTRL_BLOCKS, h->nctrl, h->d_grad + (size_t)n * h->nctrl);
+    h->launches += 2;
+    GPE_CUDA(cudaGetLastError());
+    return GPE_OK;
+}
+
+template <typename R>
+gpe_status control_gradient_t(gpe_handle* h, const double* host_u, int nsteps, const double* host_target, int K,
+                              double* loss_out, double* host_grad) {
+    typedef typename Cx<R>::T C;
+    GPE_TRY(canonicalize_t<R>(h));
+    h->w_fwd_A = false;
+    h->hb_old_valid = false;
+    const size_t fb = h->esz * h->N;
+    const int ncp = (nsteps + K - 1) / K + 1;
+    // buffers: u, grad, partials, work fields, checkpoints (kept for reuse)
+    cudaFree(h->d_u);
+    cudaFree(h->d_grad);
+    h->d_u = h->d_grad = nullptr;
+    GPE_CUDA(cudaMalloc((void**)&h->d_u, sizeof(double) * (size_t)nsteps * h->nctrl + 8));
+    GPE_CUDA(cudaMalloc((void**)&h->d_grad, sizeof(double) * (size_t)nsteps * h->nctrl + 8));
+    if (!h->d_part) GPE_CUDA(cudaMalloc((void**)&h->d_part, sizeof(double) * CTRL_BLOCKS * 64));
+    if (!h->qf) GPE_CUDA(cudaMalloc(&h->qf, sizeof(R) * h->N));
+    for (int i = 0; i < 7; ++i)
+        if (!h->adj[i]) GPE_CUDA(cudaMalloc(&h->adj[i], fb));
+    const int nstore = ncp + K + 1;
+    while ((int)h->cps.size() < nstore) {
+        void* p = nullptr;
+        GPE_CUDA(cudaMalloc(&p, fb));
+        h->cps.push_back(p);
+    }
+    GPE_CUDA(cudaMemcpyAsync(h->d_u, host_u, sizeof(double) * (size_t)nsteps * h->nctrl, cudaMemcpyHostToDevice, h->st));
+    GPE_CUDA(cudaMemcpyAsync(h->V0, h->V[0], fb, cudaMemcpyDeviceToDevice, h->st));
+    void* target = h->adj[6];
+    GPE_TRY(upload_c128_host(h, host_target, target));
+    // forward with checkpoints cps[0..ncp-1] (cps[j] = psi at step j*K)
+    GPE_CUDA(cudaMemcpyAsync(h->cps[0], h->A[0], fb, cudaMemcpyDeviceToDevice, h->st));
+    for (int n = 0; n < nsteps; ++n) {
+        GPE_TRY(ctrl_form_v<R>(h, n));
+        GPE_TRY(step_real_t<R>(h, n, 1, nullptr));
+        if ((n + 1) % K == 0 && n + 1 < nsteps)
+            GPE_CUDA(cudaMemcpyAsync(h->cps[(n + 1) / K], h->A[0], fb, cudaMemcpyDeviceToDevice, h->st));
+    }
+    // loss = 1 - |o|^2, o = sum conj(target) psi_T DV
+    k_ctrl_partials<C, R><<<CTRL_BLOCKS, 256, 0, h->st>>>(0, (const C*)target, (const C*)h->A[0], nullptr, nullptr, 0,
+                                                         h->N, h->d_part);
+    k_ctrl_final<<<1, 64, 0, h->st>>>(h->d_part, CTRL_BLOCKS, 2, h->d_grad);
+    h->launches += 2;
+    double o[2];
+    GPE_CUDA(cudaMemcpyAsync(o, h->d_grad, sizeof(o), cudaMemcpyDeviceToHost, h->st));
+    GPE_CUDA(cudaStreamSynchronize(h->st));
+    const double DV = h->cfg.dx[0] * h->cfg.dx[1] * h->cfg.dx[2];
+    o[0] *= DV;
+    o[1] *= DV;
+    if (loss_out) *loss_out = 1.0 - (o[0] * o[0] + o[1] * o[1]);
+    if (host_grad) {
+        // lambda_T = -2 o target DV
+        k_cscale<C><<<blocks_for(h->N, 256), 256, 0, h->st>>>((C*)h->adj[0], (const C*)target, -2.0 * o[0] * DV,
+                                                            -2.0 * o[1] * DV, h->N);
+        h->launches++;
+        void** seg = h->cps.data() + ncp;  // K + 1 states of one segment
+        for (int j = (nsteps - 1) / K; j >= 0; --j) {
+            const int n0 = j * K, n1 = std::min(nsteps, n0 + K);
+            GPE_CUDA(cudaMemcpyAsync(h->A[0], h->cps[j], fb, cudaMemcpyDeviceToDevice, h->st));
+            h->w_fwd_A = false;  // A was replaced: W no longer holds its transform
+            for (int n = n0; n < n1; ++n) {
+                GPE_CUDA(cudaMemcpyAsync(seg[n - n0], h->A[0], fb, cudaMemcpyDeviceToDevice, h->st));
+                if (n + 1 < n1) {
+                    GPE_TRY(ctrl_form_v<R>(h, n));
+                    GPE_TRY(step_real_t<R>(h, n, 1, nullptr));
+                }
+            }
+            for (int n = n1 - 1; n >= n0; --n) {
+                GPE_TRY(ctrl_form_v<R>(h, n));
+                GPE_TRY(ctrl_stage_args<R>(h, seg[n - n0], h->adj[3], h->adj[4], h->adj[5], n));
+                GPE_TRY(ctrl_adjoint_step<R>(h, seg[n - n0], h->adj[3], h->adj[4], h->adj[5], n));
+                GPE_TRY(ctrl_reduce_grad<R>(h, n));
+            }
+        }
+        GPE_CUDA(cudaMemcpyAsync(host_grad, h->d_grad, sizeof(double) * (size_t)nsteps * h->nctrl,
+                                 cudaMemcpyDeviceToHost, h->st));
+    }
+    // leave psi and V as they were
+    GPE_CUDA(cudaMemcpyAsync(h->A[0], h->cps[0], fb, cudaMemcpyDeviceToDevice, h->st));
+    GPE_CUDA(cudaMemcpyAsync(h->V[0], h->V0, fb, cudaMemcpyDeviceToDevice, h->st));
+    GPE_CUDA(cudaStreamSynchronize(h->st));
+    h->w_fwd_A = false;
+    return check_device_status(h);
+}
 
 // A handle holding nb instances of one configuration (nb > 1: a gpe_batch
 // group; instance i's fields start at element i*N, its parameters, scalars
@@ -1028,6 +1278,39 @@ gpe_status gpe_profile_read(gpe_handle* h, double* ms_out, long long* count_out)
         if (count_out) count_out[k] = cnt[k];
     }
     return GPE_OK;
+}
+
+gpe_status gpe_control_set_basis(gpe_handle* h, int nctrl, const double* host_G) {
+    GPE_TRY(check_handle(h));
+    if (h->ncomp != 1 || h->cfg.hamiltonian != GPE_HAM_BEC || h->nb != 1)
+        return fail(GPE_ERR_UNSUPPORTED, "the control gradient needs one component and GPE_HAM_BEC");
+    if (nctrl < 1 || nctrl > 64 || !host_G) return fail(GPE_ERR_INVALID_ARG, "nctrl must be 1..64 with a basis");
+    const size_t rs = h->prec == GPE_C64 ? 4 : 8;
+    if (h->ctrlG) cudaFree(h->ctrlG);
+    h->ctrlG = nullptr;
+    GPE_CUDA(cudaMalloc(&h->ctrlG, rs * (size_t)nctrl * h->N));
+    if (!h->V0) GPE_CUDA(cudaMalloc(&h->V0, h->esz * h->N));
+    if (rs == 8) {
+        GPE_CUDA(cudaMemcpy(h->ctrlG, host_G, 8 * (size_t)nctrl * h->N, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> g((size_t)nctrl * h->N);
+        for (size_t i = 0; i < g.size(); ++i) g[i] = (float)host_G[i];
+        GPE_CUDA(cudaMemcpy(h->ctrlG, g.data(), 4 * g.size(), cudaMemcpyHostToDevice));
+    }
+    h->nctrl = nctrl;
+    return GPE_OK;
+}
+
+gpe_status gpe_control_gradient(gpe_handle* h, const double* host_u, int nsteps, const double* host_target_c128,
+                                int checkpoint_every, double* loss_out, double* host_grad) {
+    GPE_TRY(check_handle(h));
+    if (!h->nctrl) return fail(GPE_ERR_INVALID_ARG, "no control basis (gpe_control_set_basis)");
+    if (!host_u || !host_target_c128 || nsteps < 1 || checkpoint_every < 1)
+        return fail(GPE_ERR_INVALID_ARG, "null u/target, nsteps < 1 or checkpoint_every < 1");
+    return h->prec == GPE_C64
+               ? control_gradient_t<float>(h, host_u, nsteps, host_target_c128, checkpoint_every, loss_out, host_grad)
+               : control_gradient_t<double>(h, host_u, nsteps, host_target_c128, checkpoint_every, loss_out,
+                                            host_grad);
 }
 
 // ---- batched independent instances -------------------------------------------------------

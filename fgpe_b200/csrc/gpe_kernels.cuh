@@ -37,7 +37,8 @@ enum EpiOp {
     EPI_HB = 2,      // heavy-ball imaginary step + renormalisation reductions
     EPI_APPLYH = 3,  // out <- h_mu, h_en
     EPI_OBS = 4,     // reductions of |psi|^2, Re(psi* h_mu), Re(psi* h_en)
-    EPI_RKI = 5      // imaginary-time RK4 stage
+    EPI_RKI = 5,     // imaginary-time RK4 stage
+    EPI_ADJ = 6      // adjoint of one real-time RK4 stage (control gradient)
 };
 enum SpecOp { SPEC_NONE = 0, SPEC_KIN = 1, SPEC_PX = 2 };
 // Compile-time role of an x-pass kernel: forward only, inverse + one epilogue
@@ -47,9 +48,10 @@ enum SpecOp { SPEC_NONE = 0, SPEC_KIN = 1, SPEC_PX = 2 };
 // is the same stage with the logging reductions of the last step of a chunk;
 // XK_RKF is XK_RK followed by the forward x transform of the state it just
 // wrote, which is the x-forward pass of the next stage.
+// XK_ADJ is the adjoint stage epilogue of the control gradient.
 enum XKind { XK_FWD = 0, XK_STORE = 1, XK_RK = 2, XK_HB = 3, XK_RKI = 4, XK_AH = 5, XK_FULL = 6, XK_RKO = 7,
-             XK_RKF = 8 };
-constexpr int NXKIND = 9;  // SPEC_PX: BECVPx, src/parallel.cu:283-292
+             XK_RKF = 8, XK_ADJ = 9 };
+constexpr int NXKIND = 10;  // SPEC_PX: BECVPx, src/parallel.cu:283-292
 
 constexpr int MAXQ = 6;       // reduced quantities per launch (3 per component)
 template <typename R>

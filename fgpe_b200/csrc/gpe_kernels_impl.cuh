@@ -237,6 +237,7 @@ __device__ void reduce_and_finalize(const PassArgs<R>& a, DD (&acc)[NQ], DD* red
 template <typename C>
 struct EpiIn {
     C V[2], psi[2], k[2], p0[2], xo[2];
+    C aux;  // EPI_ADJ: running control-gradient density
 };
 
 template <typename R, int EPI>
@@ -264,6 +265,14 @@ __device__ __forceinline__ EpiIn<typename Cx<R>::T> load_inputs(const PassArgs<R
                 if (a.stage > 1) {
                     in.psi[c] = a.pin[c][gi];
                     in.k[c] = a.kacc[c][gi];
+                }
+            } else if constexpr (EPI == EPI_ADJ) {
+                in.psi[c] = a.pin[c][gi];     // mu, the stage adjoint being applied
+                in.p0[c] = a.buf[0][c][gi];   // psi_s, the stage argument
+                in.k[c] = a.out[0][gi];       // lambda_{n+1}
+                if (a.stage < 4) {
+                    in.xo[c] = a.kacc[c][gi];  // running sum of J^T terms
+                    in.aux = mk(reinterpret_cast<const R*>(a.out[1])[gi], (R)0);
                 }
             } else {
                 in.psi[c] = load_psi<R>(a, ps, c, gi, cur);
@@ -395,6 +404,44 @@ __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const HamCo
                 }
             }
             return;
+        } else if constexpr (EPI == EPI_ADJ) {
+            // Reverse of one stage of the real-time RK4 step with
+            // f(psi) = -i h(psi), h = T + W + g|psi|^2 (one component):
+            //   jt = J^T mu = i (T mu + (W.re + 2 g |psi_s|^2) mu - i W.im mu) - i g psi_s^2 conj(mu)
+            //   q  += Im(conj(mu) psi_s)           (control-gradient density)
+            //   stage 4: acc = lambda + jt; 3, 2: acc += jt; 1: lambda <- acc + jt
+            //   next mu = c_re * lambda + c_im * jt   (stages 4, 3, 2)
+            const C mu = in.psi[0], ps = in.p0[0], lam = in.k[0];
+            const C Tm = T[0];
+            const R g = hc.g_mu;
+            const R n2 = ps.x * ps.x + ps.y * ps.y;
+            const R aw = V[0].x + 2 * g * n2;
+            const R Ar = Tm.x + aw * mu.x + V[0].y * mu.y;
+            const R Ai = Tm.y + aw * mu.y - V[0].y * mu.x;
+            const R s2r = ps.x * ps.x - ps.y * ps.y, s2i = 2 * ps.x * ps.y;
+            const R Br = s2r * mu.x + s2i * mu.y;
+            const R Bi = s2i * mu.x - s2r * mu.y;
+            const C jt = mk(-Ai + g * Bi, Ar - g * Br);
+            R q = mu.x * ps.y - mu.y * ps.x;
+            R* qf = reinterpret_cast<R*>(a.out[1]);
+            const int stage = a.stage;
+            C acc2;
+            if (stage == 4) {
+                acc2 = mk(lam.x + jt.x, lam.y + jt.y);
+            } else {
+                acc2 = mk(in.xo[0].x + jt.x, in.xo[0].y + jt.y);
+                q += in.aux.x;
+            }
+            qf[gi] = q;
+            if (stage == 1) {
+                a.out[0][gi] = acc2;
+            } else {
+                a.kacc[0][gi] = acc2;
+                const R cl = (R)a.c_re, cj = (R)a.c_im;
+                a.buf[1][0][gi] = mk(cl * lam.x + cj * jt.x, cl * lam.y + cj * jt.y);
+            }
+            (void)nv;
+            return;
         } else {
             // EPI_APPLYH / EPI_OBS
 #pragma unroll
@@ -470,6 +517,7 @@ __device__ __forceinline__ void epilogue_dispatch(const PassArgs<R>& a, const Ha
     else if constexpr (KIND == XK_RKO) GPE_EPI(EPI_RK, true);
     else if constexpr (KIND == XK_HB) GPE_EPI(EPI_HB, true);
     else if constexpr (KIND == XK_RKI) GPE_EPI(EPI_RKI, true);
+    else if constexpr (KIND == XK_ADJ) GPE_EPI(EPI_ADJ, false);
     else if constexpr (KIND == XK_AH) {
         // the apply-H kernel serves both EPI_APPLYH and EPI_OBS
         if (a.epi == EPI_OBS) GPE_EPI(EPI_OBS, true);
@@ -768,6 +816,7 @@ __host__ __device__ inline int xkind_of(int mode, int epi) {
         case EPI_RK: return XK_RK;  // XK_RKO when the logging reductions are wanted (see launch_xpass)
         case EPI_HB: return XK_HB;
         case EPI_RKI: return XK_RKI;
+        case EPI_ADJ: return XK_ADJ;
         default: return XK_AH;
     }
 }
@@ -777,6 +826,10 @@ cudaError_t launch_xpass(const PassArgs<R>& a, int rows, size_t smem, cudaStream
     int kind = xkind_of(a.mode, a.epi);
     if (kind == XK_RK && a.want_obs && a.stage == 4) kind = XK_RKO;
     else if (kind == XK_RK && a.fuse_fwd) kind = XK_RKF;
+    if (kind == XK_ADJ) {
+        if constexpr (NF == 1) return launch_xpass_kind<R, L, NF, XK_ADJ>(a, rows, smem, st);
+        return cudaErrorNotSupported;
+    }
     switch (kind) {
         case XK_FWD: return launch_xpass_kind<R, L, NF, XK_FWD>(a, rows, smem, st);
         case XK_STORE: return launch_xpass_kind<R, L, NF, XK_STORE>(a, rows, smem, st);

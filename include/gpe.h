@@ -186,6 +186,22 @@ gpe_status gpe_momentum_x(gpe_handle* h, int comp, double* px);
  * (CUFFT_INVERSE): the cufftExecZ2Z calls of src/baseHamiltonian.cu:89,95. */
 gpe_status gpe_fft(gpe_handle* h, int comp, int sign);
 
+/* ---- optimal-control gradient (no counterpart in the reference) ------------
+ * Real-time RK4 (the gpe_step_real scheme, one component, GPE_HAM_BEC) where
+ * step n uses the potential W_n = V + sum_k u[n*nctrl + k] G_k, and the
+ * final-state infidelity L = 1 - |o|^2, o = sum conj(target) psi(T) DV.
+ * The gradient dL/du is the discrete adjoint of the RK4 step: each stage's
+ * transpose Jacobian J^T mu = i (T + W + 2g|psi|^2) mu - i g psi^2 conj(mu)
+ * runs through the same fused FFT passes; states are recomputed from
+ * checkpoints every checkpoint_every steps (memory: about
+ * nsteps/checkpoint_every + checkpoint_every + 8 fields). */
+/* nctrl (1..64) real basis functions, host array nctrl x N (FP64). */
+gpe_status gpe_control_set_basis(gpe_handle* h, int nctrl, const double* host_G);
+/* From the handle's current psi (left unchanged, as is V): *loss_out and, if
+ * host_grad is not NULL, host_grad[n*nctrl + k] = dL/du[n*nctrl + k]. */
+gpe_status gpe_control_gradient(gpe_handle* h, const double* host_u, int nsteps, const double* host_target_c128,
+                                int checkpoint_every, double* loss_out, double* host_grad);
+
 /* ---- batched independent instances (no counterpart in the reference, whose
  * parameter sweeps are separate ./gpe runs) ----------------------------------
  * A batch holds n one-component instances that may differ in grid geometry

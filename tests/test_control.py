@@ -1,0 +1,93 @@
+"""Control gradient (gpe_control_gradient: forward RK4 with a time-dependent
+control potential, final-state infidelity, hand-written adjoint with
+checkpoints) against the FP64 adjoint restatement and central finite
+differences."""
+import numpy as np
+import pytest
+
+import adjoint_oracle as ad
+from fgpe_b200 import C64, C128, Solver, grid_axes, make_config
+
+pytestmark = pytest.mark.gpu
+
+
+def problem(prec, nsteps=24, n=32, nctrl=4, seed=5):
+    cfg = make_config((n, n, 1), (5.0, 5.0, 1.0), dt=2e-3, g=30.0, precision=prec)
+    x, y, _ = grid_axes(cfg)
+    Y, X = np.meshgrid(y, x, indexing="ij")
+    V0 = (0.5 * (X ** 2 + Y ** 2) + 0j).reshape(1, n, n)
+    rng = np.random.default_rng(seed)
+    centres = rng.uniform(-2.0, 2.0, size=(nctrl, 2))
+    G = np.stack([np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / 2.0) for cx, cy in centres]).reshape(nctrl, 1, n, n)
+    dv = cfg.dx[0] * cfg.dx[1] * cfg.dx[2]
+    psi0 = np.exp(-(X ** 2 + Y ** 2) / 2.0) * (1 + 0.05j * X)
+    psi0 = (psi0 / np.sqrt(np.sum(np.abs(psi0) ** 2) * dv)).reshape(1, n, n)
+    target = X * np.exp(-(X ** 2 + Y ** 2) / 2.0) + 0j
+    target = (target / np.sqrt(np.sum(np.abs(target) ** 2) * dv)).reshape(1, n, n)
+    u = rng.normal(0.0, 0.1, size=(nsteps, nctrl))
+    s = Solver(cfg)
+    s.set_vext(0, V0)
+    s.set_psi(0, psi0)
+    s.control_set_basis(G)
+    oracle = ad.ControlProblem(cfg, V0, G, psi0, target)
+    return s, oracle, u, target
+
+
+def rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b))
+
+
+def test_complex128_matches_oracle_and_leaves_state(gpu):
+    s, o, u, target = problem(C128)
+    before = s.get_psi(0)
+    L, grad = s.control_gradient(u, target, checkpoint_every=5)  # 24 steps: segments of 5 and a remainder
+    Lo, go = o.gradient(u)
+    assert abs(L - Lo) <= 1e-12 * abs(Lo)
+    assert rel(grad, go) <= 1e-10
+    assert np.array_equal(s.get_psi(0), before)
+    # checkpoint spacing does not change the result
+    L2, grad2 = s.control_gradient(u, target, checkpoint_every=24)
+    assert L2 == L and np.array_equal(grad2, grad)
+
+
+def test_complex64_against_oracle_and_finite_differences(gpu):
+    s64, o, u, target = problem(C64)
+    s128, _, _, _ = problem(C128)
+    L, grad = s64.control_gradient(u, target, checkpoint_every=6)
+    Lo, go = o.gradient(u)
+    assert abs(L - Lo) <= 1e-5 * abs(Lo)
+    assert rel(grad, go) <= 1e-4
+    # central differences of the complex128 forward map, h = 1e-4
+    rng = np.random.default_rng(11)
+    gmax = np.abs(go).max()
+    h = 1e-4
+    checked = 0
+    for _ in range(40):
+        n, k = rng.integers(u.shape[0]), rng.integers(u.shape[1])
+        if abs(go[n, k]) < 0.05 * gmax:
+            continue
+        up, um = u.copy(), u.copy()
+        up[n, k] += h
+        um[n, k] -= h
+        Lp, _ = s128.control_gradient(up, target, 6, want_grad=False)
+        Lm, _ = s128.control_gradient(um, target, 6, want_grad=False)
+        fd = (Lp - Lm) / (2 * h)
+        assert abs(fd - grad[n, k]) <= 1e-4 * abs(fd), (n, k, fd, grad[n, k])
+        checked += 1
+        if checked == 8:
+            break
+    assert checked >= 4
+
+
+def test_torch_function_and_driver(gpu):
+    import torch
+    from fgpe_b200.control import control_loss, optimise
+    s, o, u, target = problem(C64, nsteps=12)
+    ut = torch.tensor(u, requires_grad=True)
+    loss = control_loss(ut, s, target, 4)
+    loss.backward()
+    L, grad = s.control_gradient(u, target, 4)
+    assert float(loss) == L
+    assert np.allclose(ut.grad.numpy(), grad, rtol=0, atol=0)
+    _, losses = optimise(s, u, target, iters=4, lr=0.2, checkpoint_every=4)
+    assert losses[-1] < losses[0]
