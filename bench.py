@@ -57,8 +57,10 @@ def parse():
     p.add_argument("--ground-steps", type=int, default=3000, help="heavy-ball iterations for the initial state")
     p.add_argument("--cufft", action="store_true",
                    help="print the comparison line: cuFFT (torch.fft) 3D forward + inverse at the same grid")
-    p.add_argument("--workload", default="quench3d", choices=["quench3d", "sweep2d"],
-                   help="sweep2d: 256 batched 2D imaginary-time instances (separate JSON line)")
+    p.add_argument("--workload", default="quench3d", choices=["quench3d", "sweep2d", "control2d"],
+                   help="sweep2d: 256 batched 2D imaginary-time instances; control2d: adjoint gradient of a "
+                        "256^2 optimal-control problem (separate JSON lines)")
+    p.add_argument("--fd-components", type=int, default=32, help="control2d: finite-difference checks")
     p.add_argument("--sweep-instances", type=int, default=256)
     p.add_argument("--sweep-converge", action="store_true",
                    help="sweep2d: also run every instance to |dmu| < 1e-8 and report the iterations")
@@ -483,9 +485,22 @@ def run_sweep(args):
     number of iterations."""
     import torch
     import fgpe_b200 as gp
-    torch.cuda.set_device(0)
+    from fgpe_b200 import sweep
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
     K, W = args.steps, max(args.warmup, 3)
-    inst = sweep_instances(args.sweep_instances, gp.C64)
+    everything = sweep_instances(args.sweep_instances, gp.C64)
+    # shard by estimated cost; no data-path collective (instances are independent)
+    mine = sweep.my_instances([(n, n, 1) for (_, _, _, n, _, _) in everything], rank, world)
+    inst = [everything[i] for i in mine]
     stream = torch.cuda.Stream()
     b = gp.Batch([c for c, *_ in inst])
     b.set_stream(stream.cuda_stream)
@@ -503,6 +518,12 @@ def run_sweep(args):
     ms = e0.elapsed_time(e1)
     launches = b.launches - l0
     inst_steps = int(it.sum())
+    if dist is not None:
+        t = torch.tensor([ms, float(inst_steps)], dtype=torch.float64, device="cuda")
+        tmax = t.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        ms, inst_steps = float(tmax[0]), int(t[1])
     value = inst_steps / (ms / 1e3)
     points = sum(n * n for *_, n, _, _ in inst)
     # 45 F per RK4 imaginary step (plus its reductions), F = N*8 bytes
@@ -520,6 +541,10 @@ def run_sweep(args):
         conv = {"all_converged": bool(cv.all()), "iterations_min": int(total.min()),
                 "iterations_max": int(total.max()), "wall_s": round(time.perf_counter() - t0, 2)}
     b.close()
+    if rank != 0:
+        dist.barrier()
+        dist.destroy_process_group()
+        return
     # sequential complex128 solves, a bounded number of iterations each
     k_seq = max(3, min(20, K))
     seq_ms, seq_steps = 0.0, 0
@@ -557,11 +582,123 @@ def run_sweep(args):
                          "frac": round(alg_bytes / (ms / 1e3) / 1e9 / peak, 4), "traffic": None,
                          "model": "45 F per RK4 imaginary iteration, F = N*8 B"},
             "gpu_launches": launches, "convergence": conv}
+    if world > 1:
+        line["n_gpus"] = world
+        line["config"]["parallelism"] = "instances sharded over ranks by estimated cost (no data-path collective)"
+    print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def control_problem(precision, nsteps=2000, n=256, seed=5):
+    """2D real-time control: 256^2 on [-10,10]^2, g = 200, psi0 = ground state of
+    V0 = (x^2 + y^2)/2 (heavy ball in the same run), 16 Gaussian controls
+    exp(-|x - c_k|^2/2) on a seeded 4x4 lattice of spacing 2, u ~ N(0, 0.1)
+    piecewise constant per RK4 step (dt = 1e-3), target the dipole state
+    x |psi0| normalised (the first excited state of the trap without
+    interaction)."""
+    import fgpe_b200 as gp
+    rng = np.random.default_rng(seed)
+    prms = np.zeros(32)
+    prms[0:3] = 200.0 / (4 * PI_REF)
+    cfg = gp.make_config((n, n, 1), (10.0, 10.0, 1.0), dt=1e-3, precision=precision, prms=prms,
+                         beta=0.9, epsilon_e=1e-12)
+    x, y, _ = gp.grid_axes(cfg)
+    Y, X = np.meshgrid(y, x, indexing="ij")
+    V0 = (0.5 * (X ** 2 + Y ** 2) + 0j).reshape(1, n, n)
+    off = rng.uniform(-0.5, 0.5, size=2)
+    cs = [(-3.0 + 2.0 * i + off[0], -3.0 + 2.0 * j + off[1]) for i in range(4) for j in range(4)]
+    G = np.stack([np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / 2.0) for cx, cy in cs]).reshape(16, 1, n, n)
+    u = rng.normal(0.0, 0.1, size=(nsteps, 16))
+    return cfg, V0, G, u, X, Y
+
+
+def run_control(args):
+    """Adjoint gradient of the 256^2 control problem: gradient evaluations/s
+    (forward + adjoint with checkpoints every 50 steps), complex64; finite
+    differences of the complex128 forward on seeded components."""
+    import torch
+    import fgpe_b200 as gp
+    torch.cuda.set_device(0)
+    cfg64, V0, G, u, X, Y = control_problem(gp.C64)
+    # ground state of V0 (complex128 heavy ball), then the dipole target
+    cfgg = cfg64.copy()
+    cfgg.precision = gp.C128
+    s = gp.Solver(cfgg)
+    s.set_vext(0, V0)
+    dv = cfgg.dx[0] * cfgg.dx[1] * cfgg.dx[2]
+    p0 = np.exp(-(X ** 2 + Y ** 2) / 2.0).reshape(V0.shape) + 0j
+    s.set_psi(0, p0 / np.sqrt(np.sum(np.abs(p0) ** 2) * dv))
+    gs_iters, _ = s.step_imag(0, 4000)
+    psi0 = s.get_psi(0)
+    s.close()
+    target = X.reshape(psi0.shape) * np.abs(psi0)
+    target = target / np.sqrt(np.sum(np.abs(target) ** 2) * dv) + 0j
+    solvers = {}
+    for name, cfg in (("c64", cfg64), ("c128", cfgg)):
+        sv = gp.Solver(cfg)
+        sv.set_stream(torch.cuda.current_stream().cuda_stream)
+        sv.set_vext(0, V0)
+        sv.set_psi(0, psi0)
+        sv.control_set_basis(G)
+        solvers[name] = sv
+    s64 = solvers["c64"]
+    W = max(1, min(args.warmup, 2))
+    for _ in range(W):
+        s64.control_gradient(u, target, 50)
+    K = max(1, min(args.steps, 5))
+    torch.cuda.synchronize()
+    l0 = s64.launches
+    t0 = time.perf_counter()
+    for _ in range(K):
+        L, grad = s64.control_gradient(u, target, 50)
+    wall = (time.perf_counter() - t0) / K
+    launches = (s64.launches - l0) // K
+    t0 = time.perf_counter()
+    s64.control_gradient(u, target, 50, want_grad=False)
+    fwd = time.perf_counter() - t0
+    # finite differences of the complex128 forward map
+    rng = np.random.default_rng(7)
+    h = 1e-4
+    s128 = solvers["c128"]
+    L128, g128 = s128.control_gradient(u, target, 50)
+    errs = []
+    for _ in range(args.fd_components):
+        n, k = rng.integers(u.shape[0]), rng.integers(u.shape[1])
+        up, um = u.copy(), u.copy()
+        up[n, k] += h
+        um[n, k] -= h
+        fd = (s128.control_gradient(up, target, 50, want_grad=False)[0]
+              - s128.control_gradient(um, target, 50, want_grad=False)[0]) / (2 * h)
+        errs.append((abs(grad[n, k] - fd), abs(fd)))
+    gmax = float(np.abs(g128).max())
+    big = [e / f for e, f in errs if f > 1e-2 * gmax]
+    line = {"metric": "control-gradient evaluations/s, 256^2 x 2000 RK4 steps x 16 controls "
+                      "(complex64 + FP64 reductions)",
+            "value": round(1.0 / wall, 4), "unit": "gradients/s", "n_gpus": 1, "steps": K, "warmup": W,
+            "ms_per_step": round(1e3 * wall, 2), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded controls and lattice; ground state computed in the run)",
+            "config": {"workload": "adjoint optimal control", "grid": [256, 256], "rk4_steps": int(u.shape[0]),
+                       "controls": 16, "checkpoint_every": 50, "dt": 1e-3, "g": 200.0},
+            "loss_c64": L, "loss_c128": L128, "forward_only_s": round(fwd, 4),
+            "gradient_s": round(wall, 4), "rk4_step_equivalents_per_s": round(u.shape[0] / wall, 1),
+            "grad_rel_l2_c64_vs_c128": float(np.linalg.norm(grad - g128) / np.linalg.norm(g128)),
+            "fd": {"components": len(errs), "h": h,
+                   "max_rel_err_components_above_1pct_of_max": max(big) if big else None,
+                   "max_abs_err_over_max_grad": max(e for e, _ in errs) / gmax},
+            "ground_state_iterations": int(gs_iters), "gpu_launches_per_gradient": int(launches)}
+    for sv in solvers.values():
+        sv.close()
     print(json.dumps(line))
 
 
 def main():
     args = parse()
+    if args.workload == "control2d":
+        run_control(args)
+        return
     if args.workload == "sweep2d":
         run_sweep(args)
         return
