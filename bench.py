@@ -449,13 +449,17 @@ def run_cufft(args):
 
 
 SWEEP_SIZES = (64, 96, 128, 192, 256, 384, 512)
+SWEEP_DT = 4e-4
 
 
 def sweep_instances(n_inst, precision, seed=4):
     """Seeded 2D imaginary-time sweep: N from SWEEP_SIZES, box [-L, L]^2 with
     L = 8 sqrt(N/64), g ~ U[10, 2000], omega_y/omega_x ~ U[1, 4], RK4 in
-    imaginary time with dt = 1e-3 until |dmu| < 1e-8; Gaussian start with
-    seeded 1e-3 complex noise."""
+    imaginary time until |dmu| < 1e-8; Gaussian start with seeded 1e-3
+    complex noise.  dt = 4e-4: the largest eigenvalue of H on the 512^2 grid
+    (kinetic 2 pi^2 (kx^2 + ky^2) ~ 1.3e3 at the corner of k-space, trap
+    ~ 4.4e3 at the corner of the box for omega_y/omega_x = 4) times dt must
+    stay inside RK4's real stability interval (2.785)."""
     import fgpe_b200 as gp
     rng = np.random.default_rng(seed)
     out = []
@@ -464,7 +468,7 @@ def sweep_instances(n_inst, precision, seed=4):
         g = float(rng.uniform(10.0, 2000.0))
         aniso = float(rng.uniform(1.0, 4.0))
         L = 8.0 * np.sqrt(n / 64.0)
-        cfg = gp.make_config((n, n, 1), (L, L, 1.0), dt=1e-3, precision=precision, g=g,
+        cfg = gp.make_config((n, n, 1), (L, L, 1.0), dt=SWEEP_DT, precision=precision, g=g,
                              imag_scheme=gp.IMAG_RK4, epsilon_e=1e-8)
         x, y, _ = gp.grid_axes(cfg)
         Y, X = np.meshgrid(y, x, indexing="ij")
@@ -533,7 +537,7 @@ def run_sweep(args):
     if args.sweep_converge:
         total = it.astype(np.int64).copy()
         t0 = time.perf_counter()
-        for _ in range(200):
+        for _ in range(60):  # at most 30000 iterations
             it2, cv = b.step_imag(500)
             total += it2
             if cv.all():
@@ -572,7 +576,7 @@ def run_sweep(args):
             "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded sizes, couplings, anisotropies; Gaussian start)",
             "config": {"workload": "2D imaginary-time RK4 sweep", "instances": len(inst), "grid_counts": counts,
-                       "points_total": points, "dt": 1e-3, "epsilon_mu": 1e-8,
+                       "points_total": points, "dt": SWEEP_DT, "epsilon_mu": 1e-8,
                        "l2": "inputs larger than L2 (%.0f MB of complex64 fields)" % (5 * 8 * points / 1e6)},
             "sequential_c128": {"value": round(seq_value, 1), "unit": "instance-steps/s",
                                 "iterations_per_instance": k_seq,
