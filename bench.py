@@ -57,7 +57,7 @@ def parse():
     p.add_argument("--ground-steps", type=int, default=3000, help="heavy-ball iterations for the initial state")
     p.add_argument("--cufft", action="store_true",
                    help="print the comparison line: cuFFT (torch.fft) 3D forward + inverse at the same grid")
-    p.add_argument("--workload", default="quench3d", choices=["quench3d", "sweep2d", "control2d"],
+    p.add_argument("--workload", default="quench3d", choices=["quench3d", "sweep2d", "control2d", "imag3d"],
                    help="sweep2d: 256 batched 2D imaginary-time instances; control2d: adjoint gradient of a "
                         "256^2 optimal-control problem (separate JSON lines)")
     p.add_argument("--fd-components", type=int, default=32, help="control2d: finite-difference checks")
@@ -698,8 +698,96 @@ def run_control(args):
     print(json.dumps(line))
 
 
+def imag_case(name, precision, scheme):
+    """Imaginary-time cases: 'ground64' (64^3 on [-8,8]^3, V = r^2/2, g = 500,
+    norm 1, dt = 1e-3, stop at |dmu| < 1e-9 or 2000 steps), 'dipolar'
+    (128x128x64 on [-12,12]^2 x [-6,6], omega = (1,1,3), g = 1000, dipoles
+    along z with eps_dd = 0.8 and a spherical cut-off R = 6, dt = 5e-4, stop at
+    |dmu| < 1e-8) and 'twocomp' (96^3, g11 = 1000, g22 = 950, g12 = 900, norms
+    0.5 each, identical traps, dt = 5e-4); Gaussian starts with seeded 1e-3
+    complex noise."""
+    import fgpe_b200 as gp
+    prms = np.zeros(32)
+    if name == "ground64":
+        shape, xm, w, dt, eps, ncomp, ham = (64, 64, 64), (8.0, 8.0, 8.0), (1.0, 1.0, 1.0), 1e-3, 1e-9, 1, gp.HAM_BEC
+        prms[0:3] = 500.0 / (4 * PI_REF)
+        npart = (1.0, 1.0)
+    elif name == "dipolar":
+        shape, xm, w, dt, eps, ncomp, ham = (128, 128, 64), (12.0, 12.0, 6.0), (1.0, 1.0, 3.0), 5e-4, 1e-8, 1, \
+            gp.HAM_DIPOLAR
+        a = 1000.0 / (4 * PI_REF)
+        prms[0:3] = a
+        prms[6] = 0.8 * a
+        prms[7:10] = [0.0, 0.0, 1.0]
+        prms[10] = 6.0
+        npart = (1.0, 1.0)
+    else:
+        shape, xm, w, dt, eps, ncomp, ham = (96, 96, 96), (8.0, 8.0, 8.0), (1.0, 1.0, 1.0), 5e-4, 1e-8, 2, \
+            gp.HAM_BEC2
+        prms[0:3] = [1000.0 / (4 * PI_REF), 950.0 / (4 * PI_REF), 900.0 / (4 * PI_REF)]
+        npart = (0.5, 0.5)
+    cfg = gp.make_config(shape, xm, dt=dt, precision=precision, prms=prms, hamiltonian=ham, ncomp=ncomp,
+                         imag_scheme=scheme, beta=0.9, npart=npart, epsilon_e=eps)
+    x, y, z = gp.grid_axes(cfg)
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    V = 0.5 * ((w[0] * X) ** 2 + (w[1] * Y) ** 2 + (w[2] * Z) ** 2) + 0j
+    dv = cfg.dx[0] * cfg.dx[1] * cfg.dx[2]
+    psis = []
+    for c in range(ncomp):
+        rng = np.random.default_rng(1 + c)
+        g = np.exp(-(X ** 2 + Y ** 2 + Z ** 2) / 2.0)
+        p = g * (1 + 1e-3 * (rng.standard_normal(g.shape) + 1j * rng.standard_normal(g.shape)))
+        psis.append(p * np.sqrt(npart[c] / (np.sum(np.abs(p) ** 2) * dv)))
+    return cfg, V, psis
+
+
+def run_imag(args):
+    """Imaginary-time iterations/s of the three imaginary-time cases in each
+    form, timed with CUDA events over a bounded number of iterations, and the
+    iterations to convergence (capped) with the final mu and E."""
+    import torch
+    import fgpe_b200 as gp
+    torch.cuda.set_device(0)
+    st = torch.cuda.current_stream()
+    out = {"metric": "imaginary-time iterations/s", "unit": "iterations/s", "n_gpus": 1, "cases": {}}
+    forms = [("c128_heavyball", gp.C128, gp.IMAG_HEAVYBALL), ("c128_rk4", gp.C128, gp.IMAG_RK4),
+             ("c64_rk4", gp.C64, gp.IMAG_RK4)]
+    for name in ("ground64", "dipolar", "twocomp"):
+        res = {}
+        for form, prec, scheme in forms:
+            cfg, V, psis = imag_case(name, prec, scheme)
+            s = gp.Solver(cfg)
+            s.set_stream(st.cuda_stream)
+            for c in range(cfg.ncomp):
+                s.set_vext(c, V)
+                s.set_psi(c, psis[c])
+            s.step_imag(0, 3)
+            K = 200
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            done, _ = s.step_imag(3, K)
+            e1.record(st)
+            torch.cuda.synchronize()
+            ips = done / (e0.elapsed_time(e1) / 1e3)
+            total, conv = 3 + done, False
+            cap = 2000 if name == "ground64" else 20000
+            while total < cap and not conv:
+                d, conv = s.step_imag(total, min(2000, cap - total))
+                total += d
+            st8 = s.imag_state()
+            res[form] = {"iterations_per_s": round(ips, 1), "converged": bool(conv), "iterations": int(total),
+                         "mu": [float(st8[4 * c + 1]) for c in range(cfg.ncomp)],
+                         "E": [float(st8[4 * c + 2]) for c in range(cfg.ncomp)]}
+            s.close()
+        out["cases"][name] = res
+    print(json.dumps(out))
+
+
 def main():
     args = parse()
+    if args.workload == "imag3d":
+        run_imag(args)
+        return
     if args.workload == "control2d":
         run_control(args)
         return

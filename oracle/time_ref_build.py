@@ -7,8 +7,9 @@ takes the wall-clock difference of two runs with niter = n1 and n2, which
 cancels start-up, initial-state set-up and file output.  Status output, frame
 output and tracing are pushed beyond niter.
 
-Usage (on a GPU host):  python oracle/time_ref_build.py [--n 128] [--n1 200] [--n2 1200]
-Prints one JSON line: steps/s of the reference build's real-time RK4 loop.
+Usage (on a GPU host):  python oracle/time_ref_build.py [--n 128] [--n1 500] [--n2 5500] [--imag]
+Prints one JSON line: steps/s of the reference build's real-time RK4 loop, or
+with --imag of its imaginary-time (heavy-ball) loop.
 """
 import argparse
 import json
@@ -22,7 +23,7 @@ BIN = os.path.join(HERE, "_ref", "gpe_ref_trace")
 
 INPUT = """hamiltonian     "bec"
 outprefix       "{out}rt_"
-treal           true
+treal           {treal}
 read_vext       false
 vprefix         "{out}"
 read_psi        false
@@ -51,7 +52,7 @@ ny              {n}
 nz              {n}
 dt              0.002
 niter           {niter}
-epsilon_e       1E-15
+epsilon_e       1E-30
 itmod           100000000
 itStatMod       100000000
 trace_every     100000000
@@ -67,10 +68,10 @@ rndseed         367
 """
 
 
-def run(n, niter, work):
+def run(n, niter, work, imag=False):
     fn = os.path.join(work, f"in_{niter}.txt")
     with open(fn, "w") as f:
-        f.write(INPUT.format(out=work + "/", n=n, niter=niter))
+        f.write(INPUT.format(out=work + "/", n=n, niter=niter, treal="false" if imag else "true"))
     t0 = time.perf_counter()
     r = subprocess.run([BIN, fn], capture_output=True, text=True, timeout=1800)
     t1 = time.perf_counter()
@@ -85,17 +86,20 @@ def main():
     ap.add_argument("--n1", type=int, default=500)
     ap.add_argument("--n2", type=int, default=5500)
     ap.add_argument("--repeat", type=int, default=5)
+    ap.add_argument("--imag", action="store_true",
+                    help="time the imaginary-time (heavy-ball) loop instead of real-time RK4")
     args = ap.parse_args()
     with tempfile.TemporaryDirectory() as work:
-        run(args.n, 10, work)  # warm the driver / module load
+        run(args.n, 10, work, args.imag)  # warm the driver / module load
         diffs = []
         for _ in range(args.repeat):
-            a = run(args.n, args.n1, work)
-            b = run(args.n, args.n2, work)
+            a = run(args.n, args.n1, work, args.imag)
+            b = run(args.n, args.n2, work, args.imag)
             diffs.append((b - a) / (args.n2 - args.n1))
     diffs.sort()
     per_step = diffs[len(diffs) // 2]
     print(json.dumps({"impl": "reference CUDA build (complex128, cuFFT)", "grid": [args.n] * 3,
+                      "loop": "imaginary time (heavy ball)" if args.imag else "real-time RK4",
                       "steps_per_s": round(1.0 / per_step, 2), "ms_per_step": round(1e3 * per_step, 4),
                       "method": f"median over {args.repeat} of wall(niter={args.n2}) - wall(niter={args.n1})",
                       "samples_ms_per_step": [round(1e3 * d, 4) for d in diffs]}))
