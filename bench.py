@@ -675,9 +675,10 @@ def run_control(args):
         um[n, k] -= h
         fd = (s128.control_gradient(up, target, 50, want_grad=False)[0]
               - s128.control_gradient(um, target, 50, want_grad=False)[0]) / (2 * h)
-        errs.append((abs(grad[n, k] - fd), abs(fd)))
+        errs.append((abs(grad[n, k] - fd), abs(fd), abs(g128[n, k] - fd)))
     gmax = float(np.abs(g128).max())
-    big = [e / f for e, f in errs if f > 1e-2 * gmax]
+    big = [e / f for e, f, _ in errs if f > 1e-2 * gmax]
+    big128 = [e / f for _, f, e in errs if f > 1e-2 * gmax]
     line = {"metric": "control-gradient evaluations/s, 256^2 x 2000 RK4 steps x 16 controls "
                       "(complex64 + FP64 reductions)",
             "value": round(1.0 / wall, 4), "unit": "gradients/s", "n_gpus": 1, "steps": K, "warmup": W,
@@ -689,9 +690,10 @@ def run_control(args):
             "loss_c64": L, "loss_c128": L128, "forward_only_s": round(fwd, 4),
             "gradient_s": round(wall, 4), "rk4_step_equivalents_per_s": round(u.shape[0] / wall, 1),
             "grad_rel_l2_c64_vs_c128": float(np.linalg.norm(grad - g128) / np.linalg.norm(g128)),
-            "fd": {"components": len(errs), "h": h,
+            "fd": {"components": len(errs), "h": h, "fd_of": "complex128 forward",
                    "max_rel_err_components_above_1pct_of_max": max(big) if big else None,
-                   "max_abs_err_over_max_grad": max(e for e, _ in errs) / gmax},
+                   "max_abs_err_over_max_grad": max(e for e, _, _ in errs) / gmax,
+                   "complex128_adjoint_max_rel_err": max(big128) if big128 else None},
             "ground_state_iterations": int(gs_iters), "gpu_launches_per_gradient": int(launches)}
     for sv in solvers.values():
         sv.close()
