@@ -284,6 +284,17 @@ struct Ctx {
     C* B(int c) const { return (C*)h->B[c]; }
 };
 
+// Moving-frame term of the plugins' alg_calcHpsi (trotate): lambda = prms[11 + c],
+// applied as - (lambda/N) kx in the kinetic multiplier where the reference
+// adds alg_addVPx: heavy-ball imaginary steps, stage 4 of a one-component
+// real-time step, apply-H and the observables.
+template <typename R>
+void set_rotation(gpe_handle* h, PassArgs<R>& a, bool on) {
+    const bool plugin = h->cfg.hamiltonian != GPE_HAM_TEMPLATE;
+    for (int c = 0; c < 2; ++c)
+        a.rot[c] = (on && plugin && c < h->ncomp) ? h->cfg.prms[11 + c] / (double)h->N : 0.0;
+}
+
 template <typename R>
 PassArgs<R> base_args(gpe_handle* h) {
     typedef typename Cx<R>::T C;
@@ -512,6 +523,9 @@ gpe_status step_real_t(gpe_handle* h, int first, int nsteps, double* obs_out) {
             a.t = (s == 1) ? (double)it * dt : (s < 4) ? (it + 0.5) * dt : (double)(it + 1) * dt;
             a.want_obs = (obs_out != nullptr && j == nsteps - 1 && s == 4) ? 1 : 0;
             a.fuse_fwd = (can_fuse && !a.want_obs) ? 1 : 0;
+            // stages 1-3 use alg_calcHpsiMU, stage 4 alg_calcHpsi
+            // (src/oneComponentGPSolver.cu:170-190)
+            set_rotation<R>(h, a, s == 4 && h->ncomp == 1);
             GPE_TRY(run_chain<R>(h, a, h->nf, w_ready));
             w_ready = a.fuse_fwd != 0;
         }
@@ -567,6 +581,7 @@ gpe_status imag_issue(gpe_handle* h, int first, int nsteps) {
             a.pro = PRO_CUR;
             a.epi = EPI_HB;
             a.stage = 0;
+            set_rotation<R>(h, a, true);  // src/oneComponentGPSolver.cu:62 alg_calcHpsi
             GPE_TRY(run_chain<R>(h, a, h->nf));
         } else {
             for (int s = 1; s <= 4; ++s) {
@@ -614,6 +629,9 @@ gpe_status apply_chain_t(gpe_handle* h, int epi, double t, int comp_only, int sp
         nf = 1;
     }
     for (int q = 0; q < 4; ++q) a.out[q] = (typename Cx<R>::T*)h->O[q];
+    // alg_calcHpsi (both outputs) carries the moving-frame term, alg_Laplace
+    // and alg_calcPx do not
+    set_rotation<R>(h, a, comp_only < 0 && spec == SPEC_KIN && (epi == EPI_APPLYH || epi == EPI_OBS));
     return run_chain<R>(h, a, nf);
 }
 
@@ -1282,8 +1300,9 @@ gpe_status gpe_profile_read(gpe_handle* h, double* ms_out, long long* count_out)
 
 gpe_status gpe_control_set_basis(gpe_handle* h, int nctrl, const double* host_G) {
     GPE_TRY(check_handle(h));
-    if (h->ncomp != 1 || h->cfg.hamiltonian != GPE_HAM_BEC || h->nb != 1)
-        return fail(GPE_ERR_UNSUPPORTED, "the control gradient needs one component and GPE_HAM_BEC");
+    if (h->ncomp != 1 || h->cfg.hamiltonian != GPE_HAM_BEC || h->nb != 1 || h->cfg.prms[11] != 0)
+        return fail(GPE_ERR_UNSUPPORTED,
+                    "the control gradient needs one component, GPE_HAM_BEC and no moving-frame term");
     if (nctrl < 1 || nctrl > 64 || !host_G) return fail(GPE_ERR_INVALID_ARG, "nctrl must be 1..64 with a basis");
     const size_t rs = h->prec == GPE_C64 ? 4 : 8;
     if (h->ctrlG) cudaFree(h->ctrlG);
@@ -1449,6 +1468,8 @@ gpe_status gpe_batch_create(const gpe_config* cfgs, int n, gpe_batch** out) {
                         "batched instances share precision, hamiltonian, imag_scheme, dt, beta, epsilon_e, npart");
         if (c.prms[3] > 0 || c.prms[4] > 0 || c.prms[5] > 0)
             return fail(GPE_ERR_UNSUPPORTED, "batched instances have a time-independent coupling (prms[3..5] <= 0)");
+        if (c.prms[11] != 0 || c.prms[12] != 0)
+            return fail(GPE_ERR_UNSUPPORTED, "batched instances have no moving-frame term (prms[11..12] = 0)");
     }
     gpe_batch* b = new gpe_batch();
     b->n = n;

@@ -92,6 +92,7 @@ struct PassArgs {
     double dt, beta, lap_scale, DV, eps;
     double npart[2];
     double c_re, c_im;       // RK stage coefficient (stage 1..3 axpy; final uses c/6)
+    double rot[2];           // moving-frame term: lambda/N per component, 0 = off
 };
 
 // Strided pass tile width: x values per CTA, the largest power of two up to

@@ -89,11 +89,20 @@ __device__ __forceinline__ void spec_point(const PassArgs<R>& a, typename Cx<R>:
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
         if (f < npsi) {
+            // kinetic multiplier; with the moving-frame term (alg_addVPx,
+            // src/baseHamiltonian.cu:198-211) also - (lambda/N) kx
+            const double rl = a.rot[f < 2 ? f : 0];
             if constexpr (sizeof(R) == 8) {
-                v[f].x = (v[f].x * a.lap_scale) * k2;
-                v[f].y = (v[f].y * a.lap_scale) * k2;
+                double x = (v[f].x * a.lap_scale) * k2, y = (v[f].y * a.lap_scale) * k2;
+                if (rl != 0.0) {
+                    const double kr = a.kx[ix] * rl;
+                    x -= v[f].x * kr;
+                    y -= v[f].y * kr;
+                }
+                v[f].x = x;
+                v[f].y = y;
             } else {
-                const R fac = (R)(a.lap_scale * k2);
+                const R fac = (R)(a.lap_scale * k2 - a.kx[ix] * rl);
                 v[f].x *= fac;
                 v[f].y *= fac;
             }

@@ -210,6 +210,9 @@ BEConeComponent::BEConeComponent(const Params& par, bool run, int hamiltonian)
         hp[9] = opt_double(p, "dipole_z", 1.0);
         hp[10] = opt_double(p, "rcutoff", 0.0) / p.aho;  // same length unit as xmax
     }
+    // hamiltonians/BEC_oneComponent.cu:98-101: trotate adds alg_addVPx with
+    // lambda = 2 pi omega / (omho aho) (the template plugin has no such term)
+    if (!is_template && p.getBool("trotate")) hp[11] = 2 * pi * p.getDouble("omega") / (p.omho * p.aho);
     setHamiltonianParams(hp);
     if (!run) return;
     if (p.getBool("treal")) {
@@ -465,6 +468,12 @@ BECtwoComponent::BECtwoComponent(const Params2& par, bool run) : TwoComponentGPS
     hp[0] = p.a11;
     hp[1] = p.a22;
     hp[2] = p.a12;
+    // hamiltonians/BEC_twoComponent.cu:125-129: trotate adds alg_addVPx with
+    // lambda = 2 pi omega / (omho aho) per component
+    if (p.getBool("trotate")) {
+        hp[11] = 2 * pi * p.getDouble("omega") / (p.omho1 * p.aho1);
+        hp[12] = 2 * pi * p.getDouble("omega") / (p.omho2 * p.aho2);
+    }
     chk(gpe_set_params(h, hp), "gpe_set_params");
     if (!run) return;
     if (p.getBool("treal")) {

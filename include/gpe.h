@@ -68,7 +68,14 @@ typedef enum gpe_precision { GPE_C128 = 0, GPE_C64 = 1 } gpe_precision;
  *                   real-space cut-off radius R (0 = no cut-off).  The kernel
  *                   is 12*pi*a_dd*((k.d)^2/k^2 - 1/3) as in
  *                   src/parallel.cu:326-352 (never called there), times
- *                   1 + 3cos(kR)/(kR)^2 - 3sin(kR)/(kR)^3 with k in rad/length. */
+ *                   1 + 3cos(kR)/(kR)^2 - 3sin(kR)/(kR)^3 with k in rad/length.
+ *  Moving-frame term (the plugins' trotate option, BaseHamiltonian::alg_addVPx,
+ *  src/baseHamiltonian.cu:198-211): for every Hamiltonian but the template,
+ *  prms[11 + c] = lambda_c (2 pi omega / (omho aho) in the reference,
+ *  hamiltonians/BEC_oneComponent.cu:98-101) adds -lambda_c P_x psi_c, with
+ *  P_x psi = IFFT(kx FFT psi)/N and kx in cycles/length, exactly where the
+ *  reference's alg_calcHpsi adds it: heavy-ball imaginary steps, stage 4 of a
+ *  one-component real-time step, gpe_apply_h and gpe_observables. */
 typedef enum gpe_hamiltonian {
     GPE_HAM_BEC = 0,
     GPE_HAM_BEC2 = 1,

@@ -303,6 +303,33 @@ struct orc_solver {
         plan.exec(out, +1);
     }
 
+    // BaseHamiltonian::alg_addVPx, src/baseHamiltonian.cu:198-211 with BECVPx
+    // (src/parallel.cu:283-292) and AppendArray: aux = IFFT(kx FFT psi)
+    // (unnormalised, kx in cycles/length), then h += (-lambda/N) aux and
+    // h_en += (-lambda/N) aux.  The plugins add it inside alg_calcHpsi when
+    // trotate is set (hamiltonians/BEC_oneComponent.cu:98-101,
+    // hamiltonians/BEC_twoComponent.cu:125-129); lambda is prms[11 + c].
+    void add_vpx(int c, double lambda) {
+        std::vector<cplx>& a = aux[c];
+        std::memcpy((void*)a.data(), (const void*)psi[c].data(), sizeof(cplx) * N);
+        plan.exec(a.data(), -1);
+        const int nx = cfg.nx;
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < N; ++i) {
+            const double kx = k[0][i % nx];
+            a[i] = cplx(a[i].real() * kx, a[i].imag() * kx);
+        }
+        plan.exec(a.data(), +1);
+        const double f = (-1) * lambda / N;
+        cplx* hm = hpsi[c].data();
+        cplx* he = hpsi_en[c].data();
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < N; ++i) {
+            hm[i] = cplx(hm[i].real() + f * a[i].real(), hm[i].imag() + f * a[i].imag());
+            he[i] = cplx(he[i].real() + f * a[i].real(), he[i].imag() + f * a[i].imag());
+        }
+    }
+
     // Dipolar mean field Phi = IFFT(vdd * FFT(|psi|^2)) / N (new; see build_vdd).
     void dipolar_field(const cplx* p, std::vector<cplx>& phi) {
         phi.resize(N);
@@ -395,6 +422,9 @@ struct orc_solver {
             for (int c = 0; c < ncomp; ++c)
                 if (want_en) hpsi_en[c] = hpsi[c];
         }
+        if (want_en && ham != GPE_HAM_TEMPLATE)
+            for (int c = 0; c < ncomp; ++c)
+                if (cfg.prms[11 + c] != 0.0) add_vpx(c, cfg.prms[11 + c]);
     }
 
     // UpdateRKStep complex overload, src/parallel.cu:238-244.

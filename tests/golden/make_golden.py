@@ -35,6 +35,8 @@ CASES = [
     ("g_hb_template", REF_TRACE, 1),
     ("g_stock_2d", REF_STOCK, 1),
     ("g_stock_rt", REF_STOCK, 1),
+    ("g_stock_rot", REF_STOCK, 1),
+    ("g_stock_rot_rt", REF_STOCK, 1),
 ]
 
 
@@ -59,12 +61,16 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
     ap.add_argument("--pack-into", default=None, help="directory for the .npz fixtures (default: --out)")
+    ap.add_argument("--only", nargs="*", default=None,
+                    help="cases to run (a real-time case needs its imaginary-time case in the same call)")
     args = ap.parse_args()
     work = os.path.abspath(os.path.join(args.out, "run"))
     os.makedirs(work, exist_ok=True)
     pack = os.path.abspath(args.pack_into or args.out)
     os.makedirs(pack, exist_ok=True)
     for case, binary, nc in CASES:
+        if args.only is not None and case not in args.only:
+            continue
         src = open(os.path.join(HERE, "inputs", case + ".txt")).read()
         inp = os.path.join(work, case + ".txt")
         with open(inp, "w") as f:

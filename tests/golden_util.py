@@ -10,7 +10,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 TRACE_CASES = ["g_hb_bec", "g_hb_conv", "g_rt_quench", "g_hb_bec2", "g_rt_bec2", "g_hb_template"]
-STOCK_CASES = ["g_stock_2d", "g_stock_rt"]
+STOCK_CASES = ["g_stock_2d", "g_stock_rt", "g_stock_rot", "g_stock_rot_rt"]
+# real-time stock cases start from the psi_final of an imaginary-time case
+PREREQ = {"g_stock_rt": "g_stock_2d", "g_stock_rot_rt": "g_stock_rot"}
 
 
 def available(case):
@@ -75,6 +77,8 @@ def config(fx, tmpdir, precision=0, stock=False):
         a = o[34]
         if stock:
             prms[0] = a  # hamiltonians/BEC_oneComponent.cu:14
+            if k.get("trotate", "false") == "true":  # :98-101, lambda = 2 pi omega / (omho aho)
+                prms[11] = 2 * 3.141592653589793 * float(k["omega"]) / (o[25] * o[24])
         else:
             prms[0:3] = [a * float(k.get(f"quench_f{i}", 1.0)) for i in range(3)]
             prms[3:6] = [float(k.get(f"quench_t{i}", 0.0)) for i in (1, 2, 3)]

@@ -79,8 +79,8 @@ def test_gpe_driver_matches_stock_reference(gpu, case, tmp_path):
     root = gu.ROOT
     gpe_bin = os.path.join(root, "fgpe_b200", "gpe")
     assert os.path.exists(gpe_bin)
-    if case == "g_stock_rt":  # needs the imaginary-time run's psi_final
-        src0 = str(gu.load("g_stock_2d")["input"]).replace("@OUT@", str(tmp_path) + "/")
+    if case in gu.PREREQ:  # needs the imaginary-time run's psi_final
+        src0 = str(gu.load(gu.PREREQ[case])["input"]).replace("@OUT@", str(tmp_path) + "/")
         (tmp_path / "in0.txt").write_text(src0)
         assert subprocess.run([gpe_bin, str(tmp_path / "in0.txt")], capture_output=True).returncode == 0
     src = str(fx["input"]).replace("@OUT@", str(tmp_path) + "/")

@@ -242,3 +242,45 @@ def test_unsupported_length_rejected(gpu):
     with pytest.raises(GPEError) as e:
         Solver(make_config((14, 8, 8), 4.0))
     assert e.value.status == 2
+
+
+@pytest.mark.parametrize("prec", [C128, C64])
+def test_moving_frame_term(gpu, prec):
+    # -lambda P_x psi (the plugins' trotate option) where the reference's
+    # alg_calcHpsi adds it: heavy ball, stage 4 of real-time steps, apply-H.
+    prms = np.zeros(32)
+    prms[:3] = 30.0 / (4 * PI_REF)
+    prms[11] = 0.7
+    cfg = make_config((16, 12, 8), (5.0, 4.0, 3.0), dt=1e-3, precision=prec, prms=prms, beta=0.5)
+    g, o = pair(cfg)
+    tol = TOL[prec] if prec == C128 else 1e-5
+    gm, ge = g.apply_h(0.0, 0)
+    om, oe = o.apply_h(0.0, 0)
+    assert rel(gm, om) < TOL[prec] and rel(ge, oe) < TOL[prec]
+    assert g.step_imag(0, 12) == o.step_imag(0, 12)
+    assert rel(g.get_psi(0), o.get_psi(0)) < tol
+    assert np.allclose(g.imag_state(), o.imag_state(), rtol=tol, atol=0)
+    og = g.step_real(0, 8, want_obs=True)
+    oo = o.step_real(0, 8, want_obs=True)
+    assert rel(g.get_psi(0), o.get_psi(0)) < tol and rel(og, oo) < tol
+    # the term changes the answer (lambda = 0 does not reproduce it)
+    prms[11] = 0.0
+    cfg0 = make_config((16, 12, 8), (5.0, 4.0, 3.0), dt=1e-3, precision=prec, prms=prms, beta=0.5)
+    z, _ = pair(cfg0)
+    assert rel(z.apply_h(0.0, 0)[0], gm) > 1e-6
+
+
+def test_moving_frame_two_components(gpu):
+    prms = np.zeros(32)
+    prms[:3] = [30.0 / (4 * PI_REF), 28.5 / (4 * PI_REF), 27.0 / (4 * PI_REF)]
+    prms[11], prms[12] = 0.4, -0.6
+    cfg = make_config((16, 12, 8), (5.0, 4.0, 3.0), dt=1e-3, ncomp=2, hamiltonian=HAM_BEC2, prms=prms,
+                      npart=(0.5, 0.5), beta=0.5)
+    g, o = pair(cfg)
+    assert g.step_imag(0, 10) == o.step_imag(0, 10)
+    for c in range(2):
+        assert rel(g.get_psi(c), o.get_psi(c)) < 1e-12
+    g.step_real(0, 6)
+    o.step_real(0, 6)
+    for c in range(2):
+        assert rel(g.get_psi(c), o.get_psi(c)) < 1e-12

@@ -190,3 +190,29 @@ def test_oracle_rejects_bad_configs():
         orc.OracleSolver(make_config((8, 8, 8), 4.0, ncomp=2, hamiltonian=HAM_BEC))
     with pytest.raises(ValueError):
         orc.OracleSolver(make_config((8, 8, 8), 4.0, ncomp=1, hamiltonian=HAM_BEC2))
+
+
+def test_moving_frame_term_matches_numpy():
+    # alg_addVPx (src/baseHamiltonian.cu:198-211): h += -(lambda/N) IFFT(kx FFT psi)
+    # with the unnormalised inverse, i.e. -lambda * ifftn(kx * fftn(psi)) in numpy.
+    prms = np.zeros(32)
+    prms[:3] = 20.0 / (4 * PI_REF)
+    prms[11] = 0.9
+    cfg = make_config((12, 10, 8), (5.0, 4.0, 3.5), dt=2e-3, prms=prms)
+    V = harmonic(cfg, (1.0, 1.3, 1.7))
+    psi = gaussian(cfg, noise=0.05)
+    s = orc.OracleSolver(cfg)
+    s.set_vext(0, V)
+    s.set_psi(0, psi)
+    hm, he = s.apply_h(0.0, 0)
+    kx, ky, kz = orc.axes(cfg)[3:]
+    K2 = kz[:, None, None] ** 2 + ky[None, :, None] ** 2 + kx[None, None, :] ** 2
+    N = psi.size
+    T = np.fft.ifftn(19.739208802 / N * K2 * np.fft.fftn(psi)) * N
+    P = np.fft.ifftn(kx[None, None, :] * np.fft.fftn(psi))
+    n = np.abs(psi) ** 2
+    a = prms[2]
+    want_mu = T + (V.real + 4 * PI_REF * a * n + 1j * V.imag) * psi - 0.9 * P
+    want_en = T + (V.real + 2 * PI_REF * a * n + 1j * V.imag) * psi - 0.9 * P
+    assert np.linalg.norm(hm - want_mu) <= 1e-13 * np.linalg.norm(want_mu)
+    assert np.linalg.norm(he - want_en) <= 1e-13 * np.linalg.norm(want_en)
