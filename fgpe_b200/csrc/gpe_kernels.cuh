@@ -252,12 +252,12 @@ __device__ __forceinline__ void ham_point(int ham, int ncomp, const HamCoef<R>& 
 }
 
 template <typename R>
-__device__ __forceinline__ HamCoef<R> make_coef(const PassArgs<R>& a) {
+__device__ __forceinline__ HamCoef<R> make_coef(const PassArgs<R>& a, const double* prms) {
     HamCoef<R> hc;
-    double q = (a.ham == GPE_HAM_BEC || a.ham == GPE_HAM_DIPOLAR) ? quench_as(a.t, a.prms) : 0.0;
+    double q = (a.ham == GPE_HAM_BEC || a.ham == GPE_HAM_DIPOLAR) ? quench_as(a.t, prms) : 0.0;
     hc.g_en = (R)(2 * GPE_PI_REF * q);
     hc.g_mu = (R)(4 * GPE_PI_REF * q);
-    const double a11 = a.prms[0], a22 = a.prms[1], a12 = a.prms[2];
+    const double a11 = prms[0], a22 = prms[1], a12 = prms[2];
     hc.g11e = (R)(2 * GPE_PI_REF * a11);
     hc.g12e = (R)(2 * GPE_PI_REF * a12);
     hc.g22e = (R)(2 * GPE_PI_REF * a22);
@@ -303,11 +303,6 @@ __device__ __forceinline__ C rk_kacc_r(C k, C h) {
 
 // ---- last-block finalize ------------------------------------------------------
 // Called by every block after its own reduction (thread 0 holds acc).
-template <typename R, int NQ>
-__device__ void reduce_and_finalize(const PassArgs<R>& a, DD (&acc)[NQ], DD* red);
-
-template <typename R>
-__device__ void finalize_scalars(const PassArgs<R>& a, const double* S);
 
 // ---- kernels ----------------------------------------------------------------
 

@@ -24,31 +24,45 @@ __device__ __forceinline__ void pass_prologue_sync() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
-// Batched launch: point a's per-instance members at instance blockIdx.y and
-// return the element offset of its fields.
+// The members of one instance: for a batched launch (gpe_batch) instance
+// blockIdx.y's scalars, parameters, partial sums and field offset.  The kernel
+// parameter block itself is never modified (a modified parameter struct would
+// be copied to local memory by every thread).
+struct InstPtr {
+    DevScalars* sc;
+    const double* prms;
+    double* partials;
+    long long boff;
+};
+
 template <typename R>
-__device__ __forceinline__ long long select_instance(PassArgs<R>& a) {
-    if (a.nbatch <= 1) return 0;
-    const int inst = blockIdx.y;
-    a.sc += inst;
-    a.prms += (size_t)inst * GPE_NO_HAMIL_PARAMS;
-    a.partials += (size_t)inst * a.pstride;
-    return (long long)inst * a.bstride;
+__device__ __forceinline__ InstPtr select_instance(const PassArgs<R>& a) {
+    InstPtr p{a.sc, a.prms, a.partials, 0};
+    if (a.nbatch > 1) {
+        const int inst = blockIdx.y;
+        p.sc += inst;
+        p.prms += (size_t)inst * GPE_NO_HAMIL_PARAMS;
+        p.partials += (size_t)inst * a.pstride;
+        p.boff = (long long)inst * a.bstride;
+    }
+    return p;
 }
 
 // Lazy normalisation factors of the current / previous heavy-ball slot.
 template <typename R>
 struct PsiScale {
     double cur[2], old[2];
+    double mu[2];  // chemical potentials of the last heavy-ball step
 };
 
 template <typename R>
-__device__ __forceinline__ PsiScale<R> load_scales(const PassArgs<R>& a, int cur) {
+__device__ __forceinline__ PsiScale<R> load_scales(const DevScalars* sc, int cur) {
     PsiScale<R> s;
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
-        s.cur[c] = a.sc->scale[cur][c];
-        s.old[c] = a.sc->scale[1 - cur][c];
+        s.cur[c] = sc->scale[cur][c];
+        s.old[c] = sc->scale[1 - cur][c];
+        s.mu[c] = sc->mu[c];
     }
     return s;
 }
@@ -116,8 +130,7 @@ __device__ __forceinline__ void spec_point(const PassArgs<R>& a, typename Cx<R>:
 
 // ---- finalize (last block, thread 0) --------------------------------------------
 template <typename R>
-__device__ void finalize_scalars(const PassArgs<R>& a, const double* S) {
-    DevScalars* sc = a.sc;
+__device__ void finalize_scalars(const PassArgs<R>& a, DevScalars* sc, const double* S) {
     const int nc = a.ncomp;
     bool bad = false;
     if (a.epi == EPI_HB) {
@@ -198,18 +211,18 @@ __device__ void finalize_scalars(const PassArgs<R>& a, const double* S) {
 }
 
 template <typename R, int NQ>
-__device__ void reduce_and_finalize(const PassArgs<R>& a, DD (&acc)[NQ], DD* red) {
+__device__ void reduce_and_finalize(const PassArgs<R>& a, const InstPtr& ip, DD (&acc)[NQ], DD* red) {
     __shared__ int is_last;
     block_reduce<NQ>(acc, red);
     if (threadIdx.x == 0) {
-        double* p = a.partials + (size_t)blockIdx.x * NQ * 2;
+        double* p = ip.partials + (size_t)blockIdx.x * NQ * 2;
 #pragma unroll
         for (int q = 0; q < NQ; ++q) {
             p[2 * q] = acc[q].s;
             p[2 * q + 1] = acc[q].c;
         }
         __threadfence();
-        const unsigned int ticket = atomicAdd(&a.sc->counter, 1u);
+        const unsigned int ticket = atomicAdd(&ip.sc->counter, 1u);
         is_last = (ticket == gridDim.x - 1) ? 1 : 0;
     }
     __syncthreads();
@@ -220,7 +233,7 @@ __device__ void reduce_and_finalize(const PassArgs<R>& a, DD (&acc)[NQ], DD* red
         for (int q = 0; q < NQ; ++q) s[q] = DD{0.0, 0.0};
         const unsigned int nb = gridDim.x;
         for (unsigned int i = threadIdx.x; i < nb; i += blockDim.x) {
-            const double* p = a.partials + (size_t)i * NQ * 2;
+            const double* p = ip.partials + (size_t)i * NQ * 2;
 #pragma unroll
             for (int q = 0; q < NQ; ++q) s[q] = dd_merge(s[q], DD{__ldcg(p + 2 * q), __ldcg(p + 2 * q + 1)});
         }
@@ -229,8 +242,8 @@ __device__ void reduce_and_finalize(const PassArgs<R>& a, DD (&acc)[NQ], DD* red
             double S[NQ];
 #pragma unroll
             for (int q = 0; q < NQ; ++q) S[q] = s[q].s + s[q].c;
-            finalize_scalars(a, S);
-            a.sc->counter = 0;
+            finalize_scalars(a, ip.sc, S);
+            ip.sc->counter = 0;
             __threadfence();
         }
     }
@@ -362,7 +375,7 @@ __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const HamCo
                 const double so = ps.old[c];
                 const C xo = in.xo[c];
                 const double ox = (double)xo.x * so, oy = (double)xo.y * so;
-                const double mu = (nc == 1) ? 0 * a.sc->mu[0] : a.sc->mu[c];
+                const double mu = (nc == 1) ? 0 * ps.mu[0] : ps.mu[c];
                 const double dt = a.dt, beta = a.beta;
                 const double2 p = to_d(psi[c]);
                 const double2 h = to_d(hmu[c]);
@@ -585,8 +598,9 @@ __global__ void __launch_bounds__(256, (xpass_min_blocks<R, L, NF, KIND>())) k_x
     constexpr int RoutF = Plan<L>::out_radix(false);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     pass_prologue_sync();
-    const long long boff = select_instance(a);
-    if (a.check_done && a.sc->done) return;
+    const InstPtr ip = select_instance(a);
+    const long long boff = ip.boff;
+    if (a.check_done && ip.sc->done) return;
 
     C* X = reinterpret_cast<C*>(smem_raw);
     const unsigned b = threadIdx.x / T, t = threadIdx.x % T;
@@ -595,8 +609,8 @@ __global__ void __launch_bounds__(256, (xpass_min_blocks<R, L, NF, KIND>())) k_x
     // g0 + reg_off(e): global index of register e of this thread's line
     const long long g0 = boff + (long long)(valid ? row : 0) * L + t;
     const RowAddr<C> addr{X + b * xpad(L)};
-    const int cur = a.sc->cur_slot;
-    const PsiScale<R> ps = load_scales<R>(a, cur);
+    const int cur = ip.sc->cur_slot;
+    const PsiScale<R> ps = load_scales<R>(ip.sc, cur);
     DD acc[MAXQ];
 #pragma unroll
     for (int q = 0; q < MAXQ; ++q) acc[q] = DD{0.0, 0.0};
@@ -653,7 +667,7 @@ __global__ void __launch_bounds__(256, (xpass_min_blocks<R, L, NF, KIND>())) k_x
         }
     }
     if constexpr (KIND != XK_FWD) {
-        const HamCoef<R> hc = make_coef<R>(a);
+        const HamCoef<R> hc = make_coef<R>(a, ip.prms);
 #pragma unroll
         for (int f = 0; f < NF; ++f) line_fft_inv<L>(v[f], addr, a.tw, t);
         if (valid) epilogue_dispatch<R, NF, KIND, L, E, T, RinF>(a, hc, ps, v, g0, cur, acc);
@@ -673,7 +687,7 @@ __global__ void __launch_bounds__(256, (xpass_min_blocks<R, L, NF, KIND>())) k_x
         if constexpr (kind_reduces<KIND>()) {
             if (epi_reduces(a)) {
                 __shared__ DD red[32 * MAXQ];
-                reduce_and_finalize<R, MAXQ>(a, acc, red);
+                reduce_and_finalize<R, MAXQ>(a, ip, acc, red);
             }
         }
     }
@@ -701,8 +715,8 @@ __global__ void __launch_bounds__(256, (spass_min_blocks<R, L, NF>())) k_spass(P
     constexpr int RoutF = Plan<L>::out_radix(false);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     pass_prologue_sync();
-    const long long boff = select_instance(a);
-    if (a.check_done && a.sc->done) return;
+    const long long boff = select_instance(a).boff;
+    if (a.check_done && (a.sc + (a.nbatch > 1 ? blockIdx.y : 0))->done) return;
 
     C* X = reinterpret_cast<C*>(smem_raw);
     constexpr int tx = spass_tx(L, (int)sizeof(C));
