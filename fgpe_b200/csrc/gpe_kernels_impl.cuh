@@ -500,7 +500,7 @@ template <typename R, int NF, int EPI, bool MAYRED, int L, int E, int T, int Rr,
 __device__ __forceinline__ void epilogue_line(const PassArgs<R>& a, const HamCoef<R>& hc, const PsiScale<R>& ps,
                                               typename Cx<R>::T (&v)[NF][E], long long g0, int cur, DD* acc) {
     typedef typename Cx<R>::T C;
-    constexpr int EC0 = NF > 1 ? 1 : 2;
+    constexpr int EC0 = (NF > 1 || FUSE) ? 1 : 2;
     constexpr int EC = (E % EC0 == 0) ? EC0 : ((E % 4 == 0) ? 4 : ((E % 2 == 0) ? 2 : 1));
 #pragma unroll
     for (int e0 = 0; e0 < E; e0 += EC) {
