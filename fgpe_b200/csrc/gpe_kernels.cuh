@@ -205,7 +205,8 @@ struct HamCoef {
     R g11e, g12e, g22e, g11m, g12m, g22m;
 };
 
-template <typename R, typename C>
+// MC: largest component count the caller can have (1 when its pass carries one field).
+template <typename R, typename C, int MC = 2>
 __device__ __forceinline__ void ham_point(int ham, int ncomp, const HamCoef<R>& hc, const C* psi, const C* T,
                                           const C* V, R phi, bool want_en, C* hmu, C* hen) {
     if (ham == GPE_HAM_BEC || ham == GPE_HAM_DIPOLAR) {
@@ -220,7 +221,7 @@ __device__ __forceinline__ void ham_point(int ham, int ncomp, const HamCoef<R>& 
         rX = (V[0].x + hc.g_mu * n) + phi;
         rY = V[0].y;
         hmu[0] = mk(T[0].x + rX * px - rY * py, T[0].y + rX * py + rY * px);
-    } else if (ham == GPE_HAM_BEC2) {
+    } else if (MC > 1 && ham == GPE_HAM_BEC2) {
         const R x1 = psi[0].x, y1 = psi[0].y, x2 = psi[1].x, y2 = psi[1].y;
         const R n1 = x1 * x1 + y1 * y1, n2 = x2 * x2 + y2 * y2;
         R aX, aY;
@@ -244,7 +245,9 @@ __device__ __forceinline__ void ham_point(int ham, int ncomp, const HamCoef<R>& 
         }
         hmu[1] = mk(T[1].x + (aX * x2 - aY * y2), T[1].y + (aX * y2 + aY * x2));
     } else {
-        for (int c = 0; c < ncomp; ++c) {
+#pragma unroll
+        for (int c = 0; c < MC; ++c) {
+            if (c >= ncomp) continue;
             hmu[c] = T[c];
             if (want_en) hen[c] = T[c];
         }
@@ -291,10 +294,16 @@ template <typename C, typename R>
 __device__ __forceinline__ C rk_axpy_r(C old, R cr, R ci, C h) {
     return mk(old.x + (cr * h.x - ci * h.y), old.y + (cr * h.y + ci * h.x));
 }
+// (complex64 multiplies by the rounded 1/6 instead of dividing by 6.)
 template <typename C, typename R>
 __device__ __forceinline__ C rk_final_r(C old, R cr, R ci, C k, C h) {
     const R aX = k.x + h.x, aY = k.y + h.y;
-    return mk(old.x + (cr * aX - ci * aY) / (R)6, old.y + (cr * aY + ci * aX) / (R)6);
+    if constexpr (sizeof(R) == 8) {
+        return mk(old.x + (cr * aX - ci * aY) / (R)6, old.y + (cr * aY + ci * aX) / (R)6);
+    } else {
+        const R s = (R)(1.0 / 6.0);
+        return mk(old.x + (cr * aX - ci * aY) * s, old.y + (cr * aY + ci * aX) * s);
+    }
 }
 template <typename C>
 __device__ __forceinline__ C rk_kacc_r(C k, C h) {

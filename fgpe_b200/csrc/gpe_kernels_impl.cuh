@@ -83,13 +83,29 @@ __device__ __forceinline__ typename Cx<R>::T load_psi(const PassArgs<R>& a, cons
     return scaled(a.buf[0][c][gi], ps.cur[c]);
 }
 
+// The host launches a pass with NF = ncomp + dens fields, so a one-field pass
+// always serves one component without the dipolar density field: its
+// component counts are compile-time constants.
+template <int NF>
+__host__ __device__ constexpr int maxc_of() {
+    return NF == 1 ? 1 : 2;
+}
+template <int NF, typename R>
+__device__ __forceinline__ int ncomp_of(const PassArgs<R>& a) {
+    return NF == 1 ? 1 : a.ncomp;
+}
+template <int NF, typename R>
+__device__ __forceinline__ int npsi_of(const PassArgs<R>& a) {
+    return NF == 1 ? 1 : NF - a.dens;
+}
+
 // ---- k-space multiply ---------------------------------------------------------
 // Kinetic: the Laplace kernel of src/parallel.cu:194-205, scale*v*(kx^2+ky^2+kz^2)
 // with scale = 19.739208802/N; dipolar density: times vdd (already / N).
 template <typename R, int NF>
 __device__ __forceinline__ void spec_point(const PassArgs<R>& a, typename Cx<R>::T (&v)[NF], int ix, int iy, int iz,
                                            long long gi) {
-    const int npsi = NF - a.dens;
+    const int npsi = npsi_of<NF>(a);
     if (a.spec == SPEC_PX) {  // v * kx (BECVPx, src/parallel.cu:289-290)
         const double kxv = a.kx[ix];
 #pragma unroll
@@ -262,20 +278,23 @@ struct EpiIn {
     C aux;  // EPI_ADJ: running control-gradient density
 };
 
-template <typename R, int EPI>
+// STG: the RK stage when the caller fixed it at compile time (1; 2 for
+// stages 2-3; 4), 0 for the run-time a.stage.
+template <typename R, int EPI, int NF, int STG>
 __device__ __forceinline__ EpiIn<typename Cx<R>::T> load_inputs(const PassArgs<R>& a, const PsiScale<R>& ps,
                                                                 long long gi, int cur) {
     typedef typename Cx<R>::T C;
     EpiIn<C> in;
-    const int nc = a.ncomp;
+    const int nc = ncomp_of<NF>(a);
+    const int stage = STG ? STG : a.stage;
     if constexpr (EPI != EPI_STORE) {
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
+        for (int c = 0; c < maxc_of<NF>(); ++c) {
             if (c >= nc) continue;
             in.V[c] = a.vext[c][gi];
             if constexpr (EPI == EPI_RK) {
                 in.psi[c] = a.pin[c][gi];
-                if (a.stage > 1) {
+                if (stage > 1) {
                     in.k[c] = a.kacc[c][gi];
                     in.p0[c] = a.buf[0][c][gi];
                 }
@@ -284,7 +303,7 @@ __device__ __forceinline__ EpiIn<typename Cx<R>::T> load_inputs(const PassArgs<R
                 in.xo[c] = a.buf[1 - cur][c][gi];
             } else if constexpr (EPI == EPI_RKI) {
                 in.p0[c] = a.buf[0][c][gi];
-                if (a.stage > 1) {
+                if (stage > 1) {
                     in.psi[c] = a.pin[c][gi];
                     in.k[c] = a.kacc[c][gi];
                 }
@@ -292,7 +311,7 @@ __device__ __forceinline__ EpiIn<typename Cx<R>::T> load_inputs(const PassArgs<R
                 in.psi[c] = a.pin[c][gi];     // mu, the stage adjoint being applied
                 in.p0[c] = a.buf[0][c][gi];   // psi_s, the stage argument
                 in.k[c] = a.out[0][gi];       // lambda_{n+1}
-                if (a.stage < 4) {
+                if (stage < 4) {
                     in.xo[c] = a.kacc[c][gi];  // running sum of J^T terms
                     in.aux = mk(reinterpret_cast<const R*>(a.out[1])[gi], (R)0);
                 }
@@ -308,36 +327,37 @@ __device__ __forceinline__ EpiIn<typename Cx<R>::T> load_inputs(const PassArgs<R
 // psi component, dipolar potential field last); in: the loaded inputs.
 // For EPI_RK, nv receives the new state of each component (the value stored
 // in buf[1] for stages 1-3, in buf[0] for stage 4).
-template <typename R, int NF, int EPI, bool MAYRED = true>
+template <typename R, int NF, int EPI, bool MAYRED, int STG>
 __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const HamCoef<R>& hc, const PsiScale<R>& ps,
                                                const typename Cx<R>::T* v, const EpiIn<typename Cx<R>::T>& in,
                                                long long gi, int cur, DD* acc, typename Cx<R>::T* nv) {
     typedef typename Cx<R>::T C;
-    const int nc = a.ncomp;
+    constexpr int MC = maxc_of<NF>();
+    const int nc = ncomp_of<NF>(a);
     if constexpr (EPI == EPI_STORE) {
 #pragma unroll
         for (int f = 0; f < NF; ++f) a.w[f][gi] = v[f];
         return;
     } else {
         C T[2], psi[2], V[2], hmu[2], hen[2];
-        const R phi = a.dens ? v[NF - 1].x : (R)0;
+        const R phi = (NF > 1 && a.dens) ? v[NF - 1].x : (R)0;
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
+        for (int c = 0; c < MC; ++c) {
             if (c < nc) {
                 T[c] = v[c];
                 V[c] = in.V[c];
             }
         }
         if constexpr (EPI == EPI_RK) {
-            const int stage = a.stage;
+            const int stage = STG ? STG : a.stage;
             const bool want_en = MAYRED && (stage == 4) && a.want_obs;
 #pragma unroll
-            for (int c = 0; c < 2; ++c)
+            for (int c = 0; c < MC; ++c)
                 if (c < nc) psi[c] = in.psi[c];
-            ham_point<R, C>(a.ham, nc, hc, psi, T, V, phi, want_en, hmu, hen);
+            ham_point<R, C, MC>(a.ham, nc, hc, psi, T, V, phi, want_en, hmu, hen);
             const R cr = (R)a.c_re, ci = (R)a.c_im;
 #pragma unroll
-            for (int c = 0; c < 2; ++c) {
+            for (int c = 0; c < MC; ++c) {
                 if (c >= nc) continue;
                 const C hm = hmu[c];
                 if (stage == 1) {
@@ -366,11 +386,11 @@ __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const HamCo
             // BECUpdatePsi (src/parallel.cu:294-302) on psi = s_cur*X_cur and
             // psi_old = s_old*X_old; psi~ is written over X_old.
 #pragma unroll
-            for (int c = 0; c < 2; ++c)
+            for (int c = 0; c < MC; ++c)
                 if (c < nc) psi[c] = in.psi[c];
-            ham_point<R, C>(a.ham, nc, hc, psi, T, V, phi, true, hmu, hen);
+            ham_point<R, C, MC>(a.ham, nc, hc, psi, T, V, phi, true, hmu, hen);
 #pragma unroll
-            for (int c = 0; c < 2; ++c) {
+            for (int c = 0; c < MC; ++c) {
                 if (c >= nc) continue;
                 const double so = ps.old[c];
                 const C xo = in.xo[c];
@@ -391,19 +411,19 @@ __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const HamCo
             }
             return;
         } else if constexpr (EPI == EPI_RKI) {
-            const int stage = a.stage;
+            const int stage = STG ? STG : a.stage;
             double2 p0[2];
 #pragma unroll
-            for (int c = 0; c < 2; ++c) {
+            for (int c = 0; c < MC; ++c) {
                 if (c >= nc) continue;
                 const double s = ps.cur[c];
                 const C x = in.p0[c];
                 p0[c] = make_double2((double)x.x * s, (double)x.y * s);
                 psi[c] = (stage == 1) ? from_d<C>(p0[c]) : in.psi[c];
             }
-            ham_point<R, C>(a.ham, nc, hc, psi, T, V, phi, stage == 1, hmu, hen);
+            ham_point<R, C, MC>(a.ham, nc, hc, psi, T, V, phi, stage == 1, hmu, hen);
 #pragma unroll
-            for (int c = 0; c < 2; ++c) {
+            for (int c = 0; c < MC; ++c) {
                 if (c >= nc) continue;
                 const double2 h = to_d(hmu[c]);
                 if (stage == 1) {
@@ -469,7 +489,7 @@ __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const HamCo
 #pragma unroll
             for (int c = 0; c < 2; ++c)
                 if (c < nc) psi[c] = in.psi[c];
-            ham_point<R, C>(a.ham, nc, hc, psi, T, V, phi, true, hmu, hen);
+            ham_point<R, C, MC>(a.ham, nc, hc, psi, T, V, phi, true, hmu, hen);
             if constexpr (EPI == EPI_APPLYH) {
 #pragma unroll
                 for (int c = 0; c < 2; ++c) {
@@ -496,7 +516,7 @@ __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const HamCo
 // chunk of EC points are loaded first, then the chunk is computed and stored.
 // FUSE: v[f][e] is replaced by the new RK state of component f (and, for the
 // dipolar density field, its |psi|^2), ready for the forward x transform.
-template <typename R, int NF, int EPI, bool MAYRED, int L, int E, int T, int Rr, bool FUSE = false>
+template <typename R, int NF, int EPI, bool MAYRED, int L, int E, int T, int Rr, bool FUSE = false, int STG = 0>
 __device__ __forceinline__ void epilogue_line(const PassArgs<R>& a, const HamCoef<R>& hc, const PsiScale<R>& ps,
                                               typename Cx<R>::T (&v)[NF][E], long long g0, int cur, DD* acc) {
     typedef typename Cx<R>::T C;
@@ -506,17 +526,18 @@ __device__ __forceinline__ void epilogue_line(const PassArgs<R>& a, const HamCoe
     for (int e0 = 0; e0 < E; e0 += EC) {
         EpiIn<C> in[EC];
 #pragma unroll
-        for (int j = 0; j < EC; ++j) in[j] = load_inputs<R, EPI>(a, ps, g0 + reg_off<L, E, T, Rr>(e0 + j), cur);
+        for (int j = 0; j < EC; ++j)
+            in[j] = load_inputs<R, EPI, NF, STG>(a, ps, g0 + reg_off<L, E, T, Rr>(e0 + j), cur);
 #pragma unroll
         for (int j = 0; j < EC; ++j) {
             C tmp[NF];
 #pragma unroll
             for (int f = 0; f < NF; ++f) tmp[f] = v[f][e0 + j];
             C nv[2];
-            epilogue_point<R, NF, EPI, MAYRED>(a, hc, ps, tmp, in[j], g0 + reg_off<L, E, T, Rr>(e0 + j), cur, acc,
-                                               nv);
+            epilogue_point<R, NF, EPI, MAYRED, STG>(a, hc, ps, tmp, in[j], g0 + reg_off<L, E, T, Rr>(e0 + j), cur,
+                                                    acc, nv);
             if constexpr (FUSE) {
-                const int npsi = NF - a.dens;
+                const int npsi = npsi_of<NF>(a);
 #pragma unroll
                 for (int f = 0; f < NF; ++f) {
                     if (f < npsi) v[f][e0 + j] = nv[f < 2 ? f : 1];
@@ -534,9 +555,14 @@ __device__ __forceinline__ void epilogue_dispatch(const PassArgs<R>& a, const Ha
 #define GPE_EPI(OP, RED) epilogue_line<R, NF, OP, RED, L, E, T, Rr>(a, hc, ps, v, g0, cur, acc)
     if constexpr (KIND == XK_STORE) GPE_EPI(EPI_STORE, false);
     else if constexpr (KIND == XK_RK) GPE_EPI(EPI_RK, false);
-    else if constexpr (KIND == XK_RKF)
-        epilogue_line<R, NF, EPI_RK, false, L, E, T, Rr, true>(a, hc, ps, v, g0, cur, acc);
-    else if constexpr (KIND == XK_RKO) GPE_EPI(EPI_RK, true);
+    else if constexpr (KIND == XK_RKF) {
+        // the hot real-time kernel: one copy of the epilogue per stage class
+        if (a.stage == 1) epilogue_line<R, NF, EPI_RK, false, L, E, T, Rr, true, 1>(a, hc, ps, v, g0, cur, acc);
+        else if (a.stage < 4) epilogue_line<R, NF, EPI_RK, false, L, E, T, Rr, true, 2>(a, hc, ps, v, g0, cur, acc);
+        else epilogue_line<R, NF, EPI_RK, false, L, E, T, Rr, true, 4>(a, hc, ps, v, g0, cur, acc);
+    } else if constexpr (KIND == XK_RKO) {  // launched for stage 4 only
+        epilogue_line<R, NF, EPI_RK, true, L, E, T, Rr, false, 4>(a, hc, ps, v, g0, cur, acc);
+    }
     else if constexpr (KIND == XK_HB) GPE_EPI(EPI_HB, true);
     else if constexpr (KIND == XK_RKI) GPE_EPI(EPI_RKI, true);
     else if constexpr (KIND == XK_ADJ) GPE_EPI(EPI_ADJ, false);
@@ -582,11 +608,32 @@ __host__ __device__ constexpr int pass_min_blocks() {
 // ---- X pass -----------------------------------------------------------------------
 // One CTA = `rows` consecutive rows of the x axis, T threads per row.  Shared
 // memory: one padded exchange row per line (rows * xpad(L) elements).
-// Roles with the FP64 reductions hold more live values: one CTA fewer.
+// Roles with the FP64 reductions hold more live values: one CTA fewer.  The
+// one-field real-time RK roles fit 64 registers: one CTA more.
 template <typename R, int L, int NF, int KIND>
 __host__ __device__ constexpr int xpass_min_blocks() {
-    return kind_reduces<KIND>() && pass_min_blocks<R, L, NF>() > 1 ? pass_min_blocks<R, L, NF>() - 1
-                                                                    : pass_min_blocks<R, L, NF>();
+    return (NF == 1 && (KIND == XK_RKF || KIND == XK_RK) && pass_min_blocks<R, L, NF>() == 3)
+               ? 4
+               : (kind_reduces<KIND>() && pass_min_blocks<R, L, NF>() > 1 ? pass_min_blocks<R, L, NF>() - 1
+                                                                           : pass_min_blocks<R, L, NF>());
+}
+
+// Warms L2 with a tile's real-time RK epilogue inputs (V, the stage state
+// and, after stage 1, the accumulator and psi0: nr consecutive rows of L
+// points from global index t0) while the inverse transform runs.  On the
+// first stage of a step they come from HBM; later stages find them in L2.
+template <typename R, int NF>
+__device__ __forceinline__ void prefetch_rk_inputs(const PassArgs<R>& a, long long t0, int nr, int L) {
+    typedef typename Cx<R>::T C;
+    const unsigned lines = ((unsigned)nr * (unsigned)L * (unsigned)sizeof(C) + 127u) / 128u;
+    const unsigned nf = a.stage > 1 ? 4u : 2u;
+    const unsigned total = (unsigned)ncomp_of<NF>(a) * nf * lines;
+    for (unsigned i = threadIdx.x; i < total; i += blockDim.x) {
+        const unsigned l = i % lines, fc = i / lines, f = fc % nf, c = fc / nf;
+        const C* base = f == 0 ? a.vext[c] : (f == 1 ? a.pin[c] : (f == 2 ? a.kacc[c] : a.buf[0][c]));
+        const char* p = reinterpret_cast<const char*>(base + t0) + (size_t)l * 128u;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+    }
 }
 
 template <typename R, int L, int NF, int KIND>
@@ -601,6 +648,10 @@ __global__ void __launch_bounds__(256, (xpass_min_blocks<R, L, NF, KIND>())) k_x
     const InstPtr ip = select_instance(a);
     const long long boff = ip.boff;
     if (a.check_done && ip.sc->done) return;
+    if constexpr (KIND == XK_RKF || KIND == XK_RK || KIND == XK_RKO) {
+        const int nr = min(rows, a.nrows - (int)blockIdx.x * rows);
+        if (nr > 0) prefetch_rk_inputs<R, NF>(a, boff + (long long)blockIdx.x * rows * L, nr, L);
+    }
 
     C* X = reinterpret_cast<C*>(smem_raw);
     const unsigned b = threadIdx.x / T, t = threadIdx.x % T;
@@ -617,7 +668,7 @@ __global__ void __launch_bounds__(256, (xpass_min_blocks<R, L, NF, KIND>())) k_x
     C v[NF][E];
 
     if constexpr (KIND == XK_FWD || KIND == XK_FULL) {
-        const int npsi = NF - a.dens;
+        const int npsi = npsi_of<NF>(a);
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const long long gi = g0 + reg_off<L, E, T, RinF>(e);
