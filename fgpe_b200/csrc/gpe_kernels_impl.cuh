@@ -514,13 +514,16 @@ __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const HamCo
 
 // Epilogue of E points (register e at line position pos(e)): inputs of a
 // chunk of EC points are loaded first, then the chunk is computed and stored.
+// One-field passes take chunks of 4 points (2 for the adjoint, whose inputs
+// would spill), two-field passes 1: as many loads in flight as the register
+// budget of the launch bounds holds without spilling.
 // FUSE: v[f][e] is replaced by the new RK state of component f (and, for the
 // dipolar density field, its |psi|^2), ready for the forward x transform.
 template <typename R, int NF, int EPI, bool MAYRED, int L, int E, int T, int Rr, bool FUSE = false, int STG = 0>
 __device__ __forceinline__ void epilogue_line(const PassArgs<R>& a, const HamCoef<R>& hc, const PsiScale<R>& ps,
                                               typename Cx<R>::T (&v)[NF][E], long long g0, int cur, DD* acc) {
     typedef typename Cx<R>::T C;
-    constexpr int EC0 = (NF > 1 || FUSE) ? 1 : 2;
+    constexpr int EC0 = (NF > 1) ? 1 : ((FUSE || EPI != EPI_ADJ) ? 4 : 2);
     constexpr int EC = (E % EC0 == 0) ? EC0 : ((E % 4 == 0) ? 4 : ((E % 2 == 0) ? 2 : 1));
 #pragma unroll
     for (int e0 = 0; e0 < E; e0 += EC) {
@@ -750,11 +753,11 @@ __global__ void __launch_bounds__(256, (xpass_min_blocks<R, L, NF, KIND>())) k_x
 // b of the tile, thread t of the line); b is the fast index so that a warp
 // loads tx consecutive x values per line position.  Shared memory: the
 // exchange buffer S[pos * tx + b].
-// Strided passes hold no epilogue state: one CTA more than pass_min_blocks
-// for the short (complex64, E <= 8) lines.
+// Strided passes hold no epilogue state: two CTAs more than pass_min_blocks
+// for the short (complex64, E <= 8) lines (48 registers, no spills).
 template <typename R, int L, int NF>
 __host__ __device__ constexpr int spass_min_blocks() {
-    return pass_min_blocks<R, L, NF>() == 3 ? 4 : pass_min_blocks<R, L, NF>();
+    return pass_min_blocks<R, L, NF>() == 3 ? 5 : pass_min_blocks<R, L, NF>();
 }
 
 template <typename R, int L, int NF>
