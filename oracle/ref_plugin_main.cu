@@ -24,9 +24,24 @@
 #include "params.hpp"
 #include "params2.hpp"
 
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <string>
+
+// Wall time of the reference's own evolution loop (runRealTimeEvol /
+// runImagTimeEvol), device-synchronised on both sides, printed to stderr as
+// "ref_loop_seconds <s>" for oracle/time_ref_build.py: process start-up,
+// cuFFT plan creation and the initial-state set-up stay outside it.
+template <typename F>
+static void timed_loop(F&& run) {
+    cudaDeviceSynchronize();
+    const auto t0 = std::chrono::steady_clock::now();
+    run();
+    cudaDeviceSynchronize();
+    const auto t1 = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "ref_loop_seconds %.9f\n", std::chrono::duration<double>(t1 - t0).count());
+}
 
 namespace {
 double opt_double(const ParamsBase& p, const char* key, double dflt) {
@@ -70,8 +85,10 @@ public:
         trace = fopen((p.outpath + "trace.txt").c_str(), "w");
         output.WritePsiInit(this->psi, p.Npoints);
         output.WriteVext(this->vext, p.Npoints);
-        if (p.getBool("treal")) runRealTimeEvol();
-        else runImagTimeEvol();
+        timed_loop([&] {
+            if (p.getBool("treal")) runRealTimeEvol();
+            else runImagTimeEvol();
+        });
         fclose(trace);
     }
 
@@ -151,8 +168,10 @@ public:
         output.WritePsiInit(this->psi2, p.Npoints, "2");
         output.WriteVext(this->vext1, p.Npoints, "1");
         output.WriteVext(this->vext2, p.Npoints, "2");
-        if (p.getBool("treal")) runRealTimeEvol();
-        else runImagTimeEvol();
+        timed_loop([&] {
+            if (p.getBool("treal")) runRealTimeEvol();
+            else runImagTimeEvol();
+        });
         fclose(trace);
     }
 

@@ -2,10 +2,12 @@
 """Time the reference's own CUDA build (complex128, cuFFT) on the local GPU.
 
 Runs oracle/_ref/gpe_ref_trace (built by oracle/ref.mk from the reference
-sources; test infrastructure) on a real-time input of the headline size and
-takes the wall-clock difference of two runs with niter = n1 and n2, which
-cancels start-up, initial-state set-up and file output.  Status output, frame
-output and tracing are pushed beyond niter.
+sources; test infrastructure) on a real-time input of the headline size.  The
+binary reports the device-synchronised wall time of the reference's own
+evolution loop (ref_loop_seconds); the difference of two runs with niter = n1
+and n2 cancels what the loop does once (the initial and final copies).
+Process start-up, cuFFT plans and file output are outside the loop; status
+output, frame output and tracing are pushed beyond niter.
 
 Usage (on a GPU host):  python oracle/time_ref_build.py [--n 128] [--n1 500] [--n2 5500] [--imag]
 Prints one JSON line: steps/s of the reference build's real-time RK4 loop, or
@@ -16,7 +18,6 @@ import json
 import os
 import subprocess
 import tempfile
-import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 BIN = os.path.join(HERE, "_ref", "gpe_ref_trace")
@@ -72,12 +73,13 @@ def run(n, niter, work, imag=False):
     fn = os.path.join(work, f"in_{niter}.txt")
     with open(fn, "w") as f:
         f.write(INPUT.format(out=work + "/", n=n, niter=niter, treal="false" if imag else "true"))
-    t0 = time.perf_counter()
     r = subprocess.run([BIN, fn], capture_output=True, text=True, timeout=1800)
-    t1 = time.perf_counter()
     if r.returncode != 0:
         raise RuntimeError(f"reference build failed ({r.returncode}): {r.stderr[-500:]}")
-    return t1 - t0
+    for line in r.stderr.splitlines():
+        if line.startswith("ref_loop_seconds "):
+            return float(line.split()[1])
+    raise RuntimeError("reference build printed no ref_loop_seconds line")
 
 
 def main():
@@ -101,7 +103,8 @@ def main():
     print(json.dumps({"impl": "reference CUDA build (complex128, cuFFT)", "grid": [args.n] * 3,
                       "loop": "imaginary time (heavy ball)" if args.imag else "real-time RK4",
                       "steps_per_s": round(1.0 / per_step, 2), "ms_per_step": round(1e3 * per_step, 4),
-                      "method": f"median over {args.repeat} of wall(niter={args.n2}) - wall(niter={args.n1})",
+                      "method": f"median over {args.repeat} of loop(niter={args.n2}) - loop(niter={args.n1}), "
+                                "device-synchronised wall time of the reference's evolution loop",
                       "samples_ms_per_step": [round(1e3 * d, 4) for d in diffs]}))
 
 
