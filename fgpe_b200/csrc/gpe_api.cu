@@ -78,6 +78,10 @@ struct gpe_handle {
     DevScalars* sc = nullptr;
     double* partials = nullptr;
     void* stage128 = nullptr;  // complex128 staging (complex64 handles)
+    // complex64 single handles: low part of the real-time step state (A holds
+    // the high part), valid while only real-time steps have written A
+    void* Lo[2] = {nullptr, nullptr};
+    bool lo_valid = false;
     long long launches = 0;
     int mode = ST_CANON;
     bool hb_old_valid = true;
@@ -117,6 +121,16 @@ template <typename C>
 __global__ void k_to_c128(double2* dst, const C* src, long long n) {
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i < n) dst[i] = to_d(src[i]);
+}
+// low part of a complex128 state stored as complex64: src - hi, rounded
+__global__ void k_lo_residual(float2* lo, const float2* hi, const double2* src, long long n) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) lo[i] = make_float2((float)(src[i].x - (double)hi[i].x), (float)(src[i].y - (double)hi[i].y));
+}
+// high + low parts of a compensated complex64 state
+__global__ void k_to_c128_hilo(double2* dst, const float2* hi, const float2* lo, long long n) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = make_double2((double)hi[i].x + (double)lo[i].x, (double)hi[i].y + (double)lo[i].y);
 }
 template <typename C>
 __global__ void k_copy(C* dst, const C* src, long long n) {
@@ -468,6 +482,7 @@ gpe_status canonicalize_t(gpe_handle* h) {
     typedef typename Cx<R>::T C;
     if (h->mode == ST_CANON) return GPE_OK;
     h->w_fwd_A = false;
+    h->lo_valid = false;
     const int thr = 256;
     for (int i = 0; i < h->nb; ++i) {
         for (int c = 0; c < h->ncomp; ++c) {
@@ -498,14 +513,28 @@ gpe_status copy_field(gpe_handle* h, void* dst, const void* src) {
 }
 
 // ---- stepping ----------------------------------------------------------------------------
+// compensate: complex64 handles carry the step state as high (A) + low (Lo)
+// parts across steps and calls (rk_final_comp); off for the control
+// gradient, whose checkpoints hold A alone.
 template <typename R>
-gpe_status step_real_t(gpe_handle* h, int first, int nsteps, double* obs_out) {
+gpe_status step_real_t(gpe_handle* h, int first, int nsteps, double* obs_out, bool compensate = true) {
+    typedef typename Cx<R>::T C;
     GPE_TRY(canonicalize_t<R>(h));
     h->hb_old_valid = false;
     const double dt = h->cfg.dt;
     PassArgs<R> a = base_args<R>(h);
     a.epi = EPI_RK;
     a.pro = PRO_PIN;
+    if (sizeof(R) == 4 && h->Lo[0] != nullptr) {
+        if (compensate) {
+            if (!h->lo_valid)
+                for (int c = 0; c < h->ncomp; ++c) GPE_CUDA(cudaMemsetAsync(h->Lo[c], 0, h->esz * h->N, h->st));
+            h->lo_valid = true;
+            for (int c = 0; c < h->ncomp; ++c) a.lo[c] = (C*)h->Lo[c];
+        } else {
+            h->lo_valid = false;
+        }
+    }
     // Each stage's x-inverse epilogue also x-forward transforms the state it
     // writes (the next stage's input) unless it runs the logging reductions;
     // the next stage then starts at the strided passes.
@@ -546,6 +575,7 @@ gpe_status step_real_t(gpe_handle* h, int first, int nsteps, double* obs_out) {
 template <typename R>
 gpe_status imag_prepare(gpe_handle* h) {
     h->w_fwd_A = false;
+    h->lo_valid = false;
     const bool rk = h->cfg.imag_scheme == GPE_IMAG_RK4;
     if (rk) {
         if (h->mode == ST_HB) GPE_TRY(canonicalize_t<R>(h));
@@ -638,6 +668,7 @@ gpe_status apply_chain_t(gpe_handle* h, int epi, double t, int comp_only, int sp
 template <typename R>
 gpe_status fft_t(gpe_handle* h, int comp, int sign) {
     h->w_fwd_A = false;
+    h->lo_valid = false;
     typedef typename Cx<R>::T C;
     GPE_TRY(canonicalize_t<R>(h));
     PassArgs<R> a = base_args<R>(h);
@@ -695,16 +726,38 @@ gpe_status upload_c128_host(gpe_handle* h, const double* host, void* dst) {
     return GPE_OK;
 }
 
-gpe_status download_c128_host(gpe_handle* h, const void* src, double* host) {
+// lo: low part added to a complex64 source (the compensated state), or null.
+gpe_status download_c128_host(gpe_handle* h, const void* src, double* host, const void* lo = nullptr) {
     if (h->prec == GPE_C128) {
         GPE_CUDA(cudaMemcpyAsync(host, src, 16 * h->N, cudaMemcpyDeviceToHost, h->st));
     } else {
-        k_to_c128<float2><<<blocks_for(h->N, 256), 256, 0, h->st>>>((double2*)h->stage128, (const float2*)src, h->N);
+        if (lo)
+            k_to_c128_hilo<<<blocks_for(h->N, 256), 256, 0, h->st>>>((double2*)h->stage128, (const float2*)src,
+                                                                     (const float2*)lo, h->N);
+        else
+            k_to_c128<float2><<<blocks_for(h->N, 256), 256, 0, h->st>>>((double2*)h->stage128, (const float2*)src,
+                                                                        h->N);
         h->launches++;
         GPE_CUDA(cudaGetLastError());
         GPE_CUDA(cudaMemcpyAsync(host, h->stage128, 16 * h->N, cudaMemcpyDeviceToHost, h->st));
     }
     GPE_CUDA(cudaStreamSynchronize(h->st));
+    return GPE_OK;
+}
+
+// After psi of component comp was stored as complex64 from the complex128
+// array src (device): its rounding residual becomes the low part, so the
+// compensated state equals the input; the other components' low parts are
+// zeroed if they were not valid.
+gpe_status set_low_part(gpe_handle* h, int comp, const void* src_c128) {
+    if (!h->Lo[comp]) return GPE_OK;
+    if (!h->lo_valid)
+        for (int c = 0; c < h->ncomp; ++c) GPE_CUDA(cudaMemsetAsync(h->Lo[c], 0, h->esz * h->N, h->st));
+    k_lo_residual<<<blocks_for(h->N, 256), 256, 0, h->st>>>((float2*)h->Lo[comp], (const float2*)h->A[comp],
+                                                             (const double2*)src_c128, h->N);
+    h->launches++;
+    GPE_CUDA(cudaGetLastError());
+    h->lo_valid = true;
     return GPE_OK;
 }
 
@@ -717,7 +770,7 @@ gpe_status ensure_out_buffers(gpe_handle* h) {
 void free_all(gpe_handle* h) {
     void* ptrs[] = {h->A[0], h->A[1], h->B[0], h->B[1], h->K[0], h->K[1], h->V[0], h->V[1], h->W[0], h->W[1],
                     h->W[2], h->O[0], h->O[1], h->O[2], h->O[3], h->tw[0], h->tw[1], h->tw[2], h->kax[0],
-                    h->kax[1], h->kax[2], h->vdd, h->prms, h->sc, h->partials, h->stage128};
+                    h->kax[1], h->kax[2], h->vdd, h->prms, h->sc, h->partials, h->stage128, h->Lo[0], h->Lo[1]};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     void* cptrs[] = {h->ctrlG, h->V0, h->adj[0], h->adj[1], h->adj[2], h->adj[3], h->adj[4], h->adj[5], h->adj[6],
@@ -899,7 +952,7 @@ gpe_status control_gradient_t(gpe_handle* h, const double* host_u, int nsteps, c
     GPE_CUDA(cudaMemcpyAsync(h->cps[0], h->A[0], fb, cudaMemcpyDeviceToDevice, h->st));
     for (int n = 0; n < nsteps; ++n) {
         GPE_TRY(ctrl_form_v<R>(h, n));
-        GPE_TRY(step_real_t<R>(h, n, 1, nullptr));
+        GPE_TRY(step_real_t<R>(h, n, 1, nullptr, false));
         if ((n + 1) % K == 0 && n + 1 < nsteps)
             GPE_CUDA(cudaMemcpyAsync(h->cps[(n + 1) / K], h->A[0], fb, cudaMemcpyDeviceToDevice, h->st));
     }
@@ -929,7 +982,7 @@ gpe_status control_gradient_t(gpe_handle* h, const double* host_u, int nsteps, c
                 GPE_CUDA(cudaMemcpyAsync(seg[n - n0], h->A[0], fb, cudaMemcpyDeviceToDevice, h->st));
                 if (n + 1 < n1) {
                     GPE_TRY(ctrl_form_v<R>(h, n));
-                    GPE_TRY(step_real_t<R>(h, n, 1, nullptr));
+                    GPE_TRY(step_real_t<R>(h, n, 1, nullptr, false));
                 }
             }
             for (int n = n1 - 1; n >= n0; --n) {
@@ -1013,6 +1066,9 @@ gpe_status create_handle(const gpe_config* cfg, int nb, gpe_handle** out) {
     for (int f = 0; f < h->nf; ++f)
         if (!dmalloc(&h->W[f], fb)) return bail(GPE_ERR_OUT_OF_MEMORY);
     if (h->prec == GPE_C64 && !dmalloc(&h->stage128, 16 * h->N)) return bail(GPE_ERR_OUT_OF_MEMORY);
+    if (h->prec == GPE_C64 && nb == 1)
+        for (int c = 0; c < h->ncomp; ++c)
+            if (!dmalloc(&h->Lo[c], h->esz * h->N)) return bail(GPE_ERR_OUT_OF_MEMORY);
 
     // Twiddles, k axes, dipolar kernel, parameters, scalars, partial sums.
     std::vector<double> kax[3];
@@ -1112,12 +1168,13 @@ gpe_status gpe_set_params(gpe_handle* h, const double prms[GPE_NO_HAMIL_PARAMS])
 }
 
 gpe_status gpe_set_psi(gpe_handle* h, int comp, const double* host_c128) {
-    if (h) h->w_fwd_A = false;
+    if (h) h->w_fwd_A = h->lo_valid = false;
     GPE_TRY(check_handle(h));
     GPE_TRY(check_comp(h, comp));
     if (!host_c128) return fail(GPE_ERR_INVALID_ARG, "null psi");
     GPE_TRY(canonicalize(h));
     GPE_TRY(upload_c128_host(h, host_c128, h->A[comp]));
+    GPE_TRY(set_low_part(h, comp, h->stage128));
     GPE_CUDA(cudaMemcpyAsync(h->B[comp], h->A[comp], h->esz * h->N, cudaMemcpyDeviceToDevice, h->st));
     GPE_CUDA(cudaStreamSynchronize(h->st));
     h->hb_old_valid = true;
@@ -1125,12 +1182,13 @@ gpe_status gpe_set_psi(gpe_handle* h, int comp, const double* host_c128) {
 }
 
 gpe_status gpe_set_psi_device(gpe_handle* h, int comp, const void* dev_c128) {
-    if (h) h->w_fwd_A = false;
+    if (h) h->w_fwd_A = h->lo_valid = false;
     GPE_TRY(check_handle(h));
     GPE_TRY(check_comp(h, comp));
     if (!dev_c128) return fail(GPE_ERR_INVALID_ARG, "null psi");
     GPE_TRY(canonicalize(h));
     GPE_TRY(upload_c128_device(h, comp, dev_c128, h->A[comp]));
+    GPE_TRY(set_low_part(h, comp, dev_c128));
     GPE_CUDA(cudaMemcpyAsync(h->B[comp], h->A[comp], h->esz * h->N, cudaMemcpyDeviceToDevice, h->st));
     h->hb_old_valid = true;
     return GPE_OK;
@@ -1141,7 +1199,7 @@ gpe_status gpe_get_psi(gpe_handle* h, int comp, double* host_c128) {
     GPE_TRY(check_comp(h, comp));
     if (!host_c128) return fail(GPE_ERR_INVALID_ARG, "null output");
     GPE_TRY(canonicalize(h));
-    return download_c128_host(h, h->A[comp], host_c128);
+    return download_c128_host(h, h->A[comp], host_c128, h->lo_valid ? h->Lo[comp] : nullptr);
 }
 
 gpe_status gpe_get_psi_device(gpe_handle* h, int comp, void* dev_c128) {
@@ -1152,7 +1210,12 @@ gpe_status gpe_get_psi_device(gpe_handle* h, int comp, void* dev_c128) {
     if (h->prec == GPE_C128) {
         GPE_CUDA(cudaMemcpyAsync(dev_c128, h->A[comp], 16 * h->N, cudaMemcpyDeviceToDevice, h->st));
     } else {
-        k_to_c128<float2><<<blocks_for(h->N, 256), 256, 0, h->st>>>((double2*)dev_c128, (const float2*)h->A[comp], h->N);
+        if (h->lo_valid)
+            k_to_c128_hilo<<<blocks_for(h->N, 256), 256, 0, h->st>>>((double2*)dev_c128, (const float2*)h->A[comp],
+                                                                     (const float2*)h->Lo[comp], h->N);
+        else
+            k_to_c128<float2><<<blocks_for(h->N, 256), 256, 0, h->st>>>((double2*)dev_c128,
+                                                                        (const float2*)h->A[comp], h->N);
         h->launches++;
         GPE_CUDA(cudaGetLastError());
     }

@@ -298,6 +298,8 @@ __device__ __forceinline__ EpiIn<typename Cx<R>::T> load_inputs(const PassArgs<R
                     in.k[c] = a.kacc[c][gi];
                     in.p0[c] = a.buf[0][c][gi];
                 }
+                if constexpr (sizeof(R) == 4)
+                    if (stage == 4 && a.lo[0] != nullptr) in.xo[c] = a.lo[c][gi];
             } else if constexpr (EPI == EPI_HB) {
                 in.psi[c] = scaled(a.buf[cur][c][gi], ps.cur[c]);
                 in.xo[c] = a.buf[1 - cur][c][gi];
@@ -369,7 +371,17 @@ __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const HamCo
                     nv[c] = rk_axpy_r(in.p0[c], cr, ci, hm);
                     a.buf[1][c][gi] = nv[c];
                 } else {
-                    nv[c] = rk_final_r(in.p0[c], cr, ci, in.k[c], hm);
+                    if constexpr (sizeof(R) == 4) {
+                        if (a.lo[0] != nullptr) {
+                            C lo;
+                            nv[c] = rk_final_comp(in.p0[c], in.xo[c], cr, ci, in.k[c], hm, lo);
+                            a.lo[c][gi] = lo;
+                        } else {
+                            nv[c] = rk_final_r(in.p0[c], cr, ci, in.k[c], hm);
+                        }
+                    } else {
+                        nv[c] = rk_final_r(in.p0[c], cr, ci, in.k[c], hm);
+                    }
                     a.buf[0][c][gi] = nv[c];
                     if (MAYRED && a.want_obs) {
                         const double2 h = to_d(hm);
@@ -514,16 +526,18 @@ __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const HamCo
 
 // Epilogue of E points (register e at line position pos(e)): inputs of a
 // chunk of EC points are loaded first, then the chunk is computed and stored.
-// One-field passes take chunks of 4 points (2 for the adjoint, whose inputs
-// would spill), two-field passes 1: as many loads in flight as the register
-// budget of the launch bounds holds without spilling.
+// One-field passes take chunks of 4 points (2 for the adjoint and for the
+// complex64 RK stage 4, which also reads the low part of the state: their
+// inputs would spill), two-field passes 1: as many loads in flight as the
+// register budget of the launch bounds holds without spilling.
 // FUSE: v[f][e] is replaced by the new RK state of component f (and, for the
 // dipolar density field, its |psi|^2), ready for the forward x transform.
 template <typename R, int NF, int EPI, bool MAYRED, int L, int E, int T, int Rr, bool FUSE = false, int STG = 0>
 __device__ __forceinline__ void epilogue_line(const PassArgs<R>& a, const HamCoef<R>& hc, const PsiScale<R>& ps,
                                               typename Cx<R>::T (&v)[NF][E], long long g0, int cur, DD* acc) {
     typedef typename Cx<R>::T C;
-    constexpr int EC0 = (NF > 1) ? 1 : ((FUSE || EPI != EPI_ADJ) ? 4 : 2);
+    constexpr bool LO = EPI == EPI_RK && sizeof(R) == 4 && (STG == 4 || STG == 0);  // may read the low part
+    constexpr int EC0 = (NF > 1) ? 1 : ((EPI == EPI_ADJ || LO) ? 2 : 4);
     constexpr int EC = (E % EC0 == 0) ? EC0 : ((E % 4 == 0) ? 4 : ((E % 2 == 0) ? 2 : 1));
 #pragma unroll
     for (int e0 = 0; e0 < E; e0 += EC) {
@@ -622,18 +636,20 @@ __host__ __device__ constexpr int xpass_min_blocks() {
 }
 
 // Warms L2 with a tile's real-time RK epilogue inputs (V, the stage state
-// and, after stage 1, the accumulator and psi0: nr consecutive rows of L
-// points from global index t0) while the inverse transform runs.  On the
-// first stage of a step they come from HBM; later stages find them in L2.
+// and, after stage 1, the accumulator and psi0, at stage 4 the low part of
+// psi0: nr consecutive rows of L points from global index t0) while the
+// inverse transform runs.  On the first stage of a step they come from HBM;
+// later stages find them in L2.
 template <typename R, int NF>
 __device__ __forceinline__ void prefetch_rk_inputs(const PassArgs<R>& a, long long t0, int nr, int L) {
     typedef typename Cx<R>::T C;
     const unsigned lines = ((unsigned)nr * (unsigned)L * (unsigned)sizeof(C) + 127u) / 128u;
-    const unsigned nf = a.stage > 1 ? 4u : 2u;
+    const unsigned nf = a.stage > 1 ? ((a.stage == 4 && a.lo[0] != nullptr) ? 5u : 4u) : 2u;
     const unsigned total = (unsigned)ncomp_of<NF>(a) * nf * lines;
     for (unsigned i = threadIdx.x; i < total; i += blockDim.x) {
         const unsigned l = i % lines, fc = i / lines, f = fc % nf, c = fc / nf;
-        const C* base = f == 0 ? a.vext[c] : (f == 1 ? a.pin[c] : (f == 2 ? a.kacc[c] : a.buf[0][c]));
+        const C* base = f == 0 ? a.vext[c]
+                               : (f == 1 ? a.pin[c] : (f == 2 ? a.kacc[c] : (f == 3 ? a.buf[0][c] : a.lo[c])));
         const char* p = reinterpret_cast<const char*>(base + t0) + (size_t)l * 128u;
         asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
     }

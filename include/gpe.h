@@ -56,7 +56,13 @@ typedef enum gpe_status {
  *  GPE_C64 : complex64 fields, FFT butterflies and real-time RK4 stage
  *            updates in FP32; norm, energy, chemical potential, the
  *            imaginary-time update, renormalisation and the convergence
- *            test stay FP64 (compensated sums). */
+ *            test stay FP64 (compensated sums).  Between real-time steps
+ *            the state is carried as float32 high + low parts (error-free
+ *            sum at the last stage), so its rounding does not accumulate;
+ *            gpe_set_psi stores the complex128 input's rounding residual as
+ *            the low part and gpe_get_psi returns the sum.  Imaginary-time
+ *            steps, gpe_fft and the control gradient use the high part
+ *            alone and drop the low part. */
 typedef enum gpe_precision { GPE_C128 = 0, GPE_C64 = 1 } gpe_precision;
 
 /* Which Hamiltonian plugin supplies the pointwise term.

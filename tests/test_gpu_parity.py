@@ -102,7 +102,10 @@ def test_real_time_call_splitting(gpu, prec, shape):
     # input; a later call reuses that transform unless something else ran in
     # between.  One call of 6 steps, 6 calls of 1 step, and calls with other
     # operations (set_psi of the same state, observables) in between must
-    # give the same bits.
+    # give the same bits.  (complex64 carries the state as float32 high and
+    # low parts; get_psi returns their complex128 sum, from which set_psi
+    # cannot always recover the same pair of floats, so there the set_psi
+    # path agrees to 1e-7 instead of bitwise.)
     prms = np.zeros(32)
     prms[:6] = [30.0 / (4 * PI_REF), 33.0 / (4 * PI_REF), 36.0 / (4 * PI_REF), 0.0, 0.003, 0.006]
     cfg = make_config(shape, (5.0, 4.0, 3.0), dt=1e-3, precision=prec, prms=prms)
@@ -121,9 +124,57 @@ def test_real_time_call_splitting(gpu, prec, shape):
     o.step_real(0, 6)
     p1 = g1.get_psi(0)
     assert np.array_equal(p1, g2.get_psi(0))
-    assert np.array_equal(p1, g3.get_psi(0))
+    if prec == C128:
+        assert np.array_equal(p1, g3.get_psi(0))
+    else:
+        assert rel(g3.get_psi(0), p1) < 1e-7
     tol = TOL[prec] if prec == C128 else 1e-5
     assert rel(p1, o.get_psi(0)) < tol
+
+
+def test_complex64_compensated_state(gpu):
+    # complex64 carries the real-time step state as float32 high + low parts
+    # (an error-free TwoSum at stage 4), across calls.  Rounding the state to
+    # float32 every step would random-walk the norm by ~1e-7 over these 2000
+    # steps; compensated, what is left comes from the float32 transforms and
+    # pointwise terms (measured 1.5e-9 in the norm, 4e-9 in E on a B200).
+    prms = np.zeros(32)
+    prms[:3] = 500.0 / (4 * PI_REF)
+    cfg64 = make_config((32, 32, 32), 8.0, dt=5e-4, precision=C64, prms=prms)
+    cfg128 = make_config((32, 32, 32), 8.0, dt=5e-4, precision=C128, prms=prms)
+    psi = gaussian(cfg64, width=1.5, seed=3, noise=1e-3)
+    s64, s128 = Solver(cfg64), Solver(cfg128)
+    for s in (s64, s128):
+        s.set_vext(0, harmonic(cfg64))
+        s.set_psi(0, psi)
+    # set_psi keeps the complex128 input exactly (rounding residual as the low part)
+    assert rel(s64.get_psi(0), psi) < 1e-13
+    o0 = s128.observables(0.0)
+    for k in range(4):
+        ob64 = s64.step_real(500 * k, 500, want_obs=True)
+        ob128 = s128.step_real(500 * k, 500, want_obs=True)
+    assert abs(ob128[0] / o0[0] - 1) < 1e-9
+    assert abs(ob64[0] / o0[0] - 1) < 1e-8
+    assert abs(ob64[2] / ob128[2] - 1) < 3e-8
+    assert rel(s64.get_psi(0), s128.get_psi(0)) < 2e-6
+
+
+def test_complex64_low_part_reset(gpu):
+    # Any operation that rewrites the state outside the real-time steps drops
+    # the low part: after imaginary-time steps, real-time stepping continues
+    # exactly as on a fresh handle given the same state.
+    prms = np.zeros(32)
+    prms[:3] = 30.0 / (4 * PI_REF)
+    cfg = make_config((16, 16, 16), 5.0, dt=1e-3, precision=C64, prms=prms)
+    g1, _ = pair(cfg)
+    g1.step_real(0, 10)
+    g1.step_imag(0, 5)
+    g2 = Solver(cfg)
+    g2.set_vext(0, harmonic(cfg, (1.0, 1.2, 1.5)))
+    g2.set_psi(0, g1.get_psi(0))
+    g1.step_real(0, 10)
+    g2.step_real(0, 10)
+    assert np.array_equal(g1.get_psi(0), g2.get_psi(0))
 
 
 @pytest.mark.parametrize("prec", [C128, C64])
