@@ -73,6 +73,7 @@ struct gpe_handle {
     void* O[4] = {nullptr, nullptr, nullptr, nullptr};
     void* tw[3] = {nullptr, nullptr, nullptr};
     double* kax[3] = {nullptr, nullptr, nullptr};
+    float* k2s[3] = {nullptr, nullptr, nullptr};  // complex64: lap_scale * k^2 per axis
     void* vdd = nullptr;
     double* prms = nullptr;
     DevScalars* sc = nullptr;
@@ -331,6 +332,7 @@ PassArgs<R> base_args(gpe_handle* h) {
     a.kx = h->kax[0];
     a.ky = h->kax[1];
     a.kz = h->kax[2];
+    for (int d = 0; d < 3; ++d) a.k2s[d] = h->k2s[d];
     a.vdd = (const R*)h->vdd;
     a.prms = h->prms;
     a.sc = h->sc;
@@ -770,7 +772,8 @@ gpe_status ensure_out_buffers(gpe_handle* h) {
 void free_all(gpe_handle* h) {
     void* ptrs[] = {h->A[0], h->A[1], h->B[0], h->B[1], h->K[0], h->K[1], h->V[0], h->V[1], h->W[0], h->W[1],
                     h->W[2], h->O[0], h->O[1], h->O[2], h->O[3], h->tw[0], h->tw[1], h->tw[2], h->kax[0],
-                    h->kax[1], h->kax[2], h->vdd, h->prms, h->sc, h->partials, h->stage128, h->Lo[0], h->Lo[1]};
+                    h->kax[1], h->kax[2], h->vdd, h->prms, h->sc, h->partials, h->stage128, h->Lo[0], h->Lo[1],
+                    h->k2s[0], h->k2s[1], h->k2s[2]};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     void* cptrs[] = {h->ctrlG, h->V0, h->adj[0], h->adj[1], h->adj[2], h->adj[3], h->adj[4], h->adj[5], h->adj[6],
@@ -1076,6 +1079,13 @@ gpe_status create_handle(const gpe_config* cfg, int nb, gpe_handle** out) {
     for (int d = 0; d < 3; ++d) {
         if (!dmalloc((void**)&h->kax[d], sizeof(double) * L3[d])) return bail(GPE_ERR_OUT_OF_MEMORY);
         cudaMemcpy(h->kax[d], kax[d].data(), sizeof(double) * L3[d], cudaMemcpyHostToDevice);
+        if (h->prec == GPE_C64) {
+            std::vector<float> k2s(L3[d]);
+            const double lap_scale = 19.739208802 / (double)h->N;  // src/parallel.cu:199
+            for (int i = 0; i < L3[d]; ++i) k2s[i] = (float)(lap_scale * kax[d][i] * kax[d][i]);
+            if (!dmalloc((void**)&h->k2s[d], sizeof(float) * L3[d])) return bail(GPE_ERR_OUT_OF_MEMORY);
+            cudaMemcpy(h->k2s[d], k2s.data(), sizeof(float) * L3[d], cudaMemcpyHostToDevice);
+        }
         if (h->prec == GPE_C128) {
             std::vector<double2> tw;
             host_twiddles(L3[d], tw);

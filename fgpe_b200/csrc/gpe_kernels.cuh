@@ -83,6 +83,7 @@ struct PassArgs {
     const double* kx;
     const double* ky;
     const double* kz;
+    const float* k2s[3];     // complex64: lap_scale * k^2 per axis, rounded to float (null for complex128)
     const R* vdd;            // dipolar kernel / N (spectral order) or null
     const double* prms;      // d_h_params
     DevScalars* sc;

@@ -115,7 +115,6 @@ __device__ __forceinline__ void spec_point(const PassArgs<R>& a, typename Cx<R>:
         }
         return;
     }
-    const double k2 = a.kx[ix] * a.kx[ix] + a.ky[iy] * a.ky[iy] + a.kz[iz] * a.kz[iz];
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
         if (f < npsi) {
@@ -123,6 +122,7 @@ __device__ __forceinline__ void spec_point(const PassArgs<R>& a, typename Cx<R>:
             // src/baseHamiltonian.cu:198-211) also - (lambda/N) kx
             const double rl = a.rot[f < 2 ? f : 0];
             if constexpr (sizeof(R) == 8) {
+                const double k2 = a.kx[ix] * a.kx[ix] + a.ky[iy] * a.ky[iy] + a.kz[iz] * a.kz[iz];
                 double x = (v[f].x * a.lap_scale) * k2, y = (v[f].y * a.lap_scale) * k2;
                 if (rl != 0.0) {
                     const double kr = a.kx[ix] * rl;
@@ -132,7 +132,15 @@ __device__ __forceinline__ void spec_point(const PassArgs<R>& a, typename Cx<R>:
                 v[f].x = x;
                 v[f].y = y;
             } else {
-                const R fac = (R)(a.lap_scale * k2 - a.kx[ix] * rl);
+                // complex64: the per-axis float tables of lap_scale * k^2
+                // (FP64 only with the moving-frame term)
+                R fac;
+                if (rl == 0.0) {
+                    fac = (a.k2s[0][ix] + a.k2s[1][iy]) + a.k2s[2][iz];
+                } else {
+                    const double k2 = a.kx[ix] * a.kx[ix] + a.ky[iy] * a.ky[iy] + a.kz[iz] * a.kz[iz];
+                    fac = (R)(a.lap_scale * k2 - a.kx[ix] * rl);
+                }
                 v[f].x *= fac;
                 v[f].y *= fac;
             }
