@@ -95,6 +95,11 @@ def lib() -> ctypes.CDLL:
         "gpe_apply_h": (c_int, [H, c_double, c_int, P, P]),
         "gpe_observables": (c_int, [H, c_double, P]),
         "gpe_fft": (c_int, [H, c_int, c_int]),
+        "gpe_momentum_x": (c_int, [H, c_int, P]),
+        "gpe_average_cos": (c_int, [H, c_int, P]),
+        "gpe_average_cos2": (c_int, [H, c_int, P]),
+        "gpe_relative_phase": (c_int, [H, P]),
+        "gpe_dsz_dt": (c_int, [H, P]),
         "gpe_sync": (c_int, [H]),
         "gpe_kernel_launches": (c_longlong, [H]),
         "gpe_profile_enable": (c_int, [H, c_int]),
@@ -304,6 +309,31 @@ class Solver:
 
     def fft(self, comp: int, sign: int) -> None:
         _check(lib().gpe_fft(self._h, comp, sign))
+
+    def _scalar(self, name: str, *args) -> float:
+        out = c_double(0.0)
+        _check(getattr(lib(), name)(self._h, *args, byref(out)))
+        return out.value
+
+    def momentum_x(self, comp: int = 0) -> float:
+        """sum Re(conj(psi) P_x psi) DV before the plugin's division (alg_calcPx)."""
+        return self._scalar("gpe_momentum_x", comp)
+
+    def average_cos(self, comp: int = 0) -> float:
+        """sum cos(2 pi x/L) |psi_comp|^2 DV (alg_calcCos; divide by the norm for <cos>)."""
+        return self._scalar("gpe_average_cos", comp)
+
+    def average_cos2(self, sign: int = 1) -> float:
+        """sum cos(2 pi x/L) |psi_0 + sign psi_1|^2 DV."""
+        return self._scalar("gpe_average_cos2", sign)
+
+    def relative_phase(self) -> float:
+        """sum (arg psi_0 - arg psi_1) DV."""
+        return self._scalar("gpe_relative_phase")
+
+    def dsz_dt(self) -> float:
+        """sum sqrt(n_0 n_1) sin(arg psi_0 - arg psi_1) DV."""
+        return self._scalar("gpe_dsz_dt")
 
     def sync(self) -> None:
         _check(lib().gpe_sync(self._h))

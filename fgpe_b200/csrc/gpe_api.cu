@@ -74,6 +74,7 @@ struct gpe_handle {
     void* tw[3] = {nullptr, nullptr, nullptr};
     double* kax[3] = {nullptr, nullptr, nullptr};
     float* k2s[3] = {nullptr, nullptr, nullptr};  // complex64: lap_scale * k^2 per axis
+    double* obs_part = nullptr;                    // OBS_BLOCKS partial sums + the result
     void* vdd = nullptr;
     double* prms = nullptr;
     DevScalars* sc = nullptr;
@@ -220,6 +221,55 @@ __global__ void k_ctrl_partials(int mode, const C* a, const C* b, const R* q, co
         __syncthreads();
     }
 }
+// ---- logging-cadence observables ----------------------------------------------------
+// Per-block FP64 (Neumaier) sums of a pointwise quantity of one or two fields:
+//  OBS_COS   cos(2 pi x/L) |a|^2               CalcAverageCos, src/parallel.cu:535-561
+//  OBS_COS2  cos(2 pi x/L) |a + sign b|^2      CalcAverageCos, src/parallel.cu:739-771
+//  OBS_PHASE atan2(a) - atan2(b)               CalculateRelativePhase, src/parallel.cu:774-802
+//  OBS_DSZ   sqrt(|a|^2 |b|^2) sin(phase)      CalculateDszDt, src/parallel.cu:805-839
+// x[ix] = -XMAX + (ix + 1/2) DX (src/baseHamiltonian.cu:25-51), ix = i % nx.
+enum { OBS_COS = 0, OBS_COS2 = 1, OBS_PHASE = 2, OBS_DSZ = 3 };
+constexpr int OBS_BLOCKS = 128;
+template <typename C>
+__global__ void k_obs_partials(int kind, const C* a, const C* b, double sign, double xmax, double dx, double L,
+                               int nx, long long n, double* part) {
+    __shared__ double sh_s[256], sh_c[256];
+    double s = 0.0, comp = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double ax = a[i].x, ay = a[i].y;
+        double v;
+        if (kind == OBS_COS || kind == OBS_COS2) {
+            const double x = -xmax + (double)(i % nx) * dx + 0.5 * dx;
+            double px = ax, py = ay;
+            if (kind == OBS_COS2) {
+                px += sign * (double)b[i].x;
+                py += sign * (double)b[i].y;
+            }
+            v = cos(2.0 * 3.141592653589793 * x / L) * (px * px + py * py);
+        } else {
+            const double bx = b[i].x, by = b[i].y;
+            const double ph = atan2(ay, ax) - atan2(by, bx);
+            v = (kind == OBS_PHASE) ? ph : sqrt((ax * ax + ay * ay) * (bx * bx + by * by)) * sin(ph);
+        }
+        const double t = s + v;  // Neumaier
+        comp += (fabs(s) >= fabs(v)) ? (s - t) + v : (v - t) + s;
+        s = t;
+    }
+    sh_s[threadIdx.x] = s;
+    sh_c[threadIdx.x] = comp;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ts = 0.0, tc = 0.0;
+        for (int k = 0; k < (int)blockDim.x; ++k) {
+            const double v = sh_s[k];
+            const double t = ts + v;
+            tc += ((fabs(ts) >= fabs(v)) ? (ts - t) + v : (v - t) + ts) + sh_c[k];
+            ts = t;
+        }
+        part[blockIdx.x] = ts + tc;
+    }
+}
+
 // out[k] = sum over blocks of part[b][k], block order.
 __global__ void k_ctrl_final(const double* part, int nblocks, int nv, double* out) {
     const int k = threadIdx.x;
@@ -773,7 +823,7 @@ void free_all(gpe_handle* h) {
     void* ptrs[] = {h->A[0], h->A[1], h->B[0], h->B[1], h->K[0], h->K[1], h->V[0], h->V[1], h->W[0], h->W[1],
                     h->W[2], h->O[0], h->O[1], h->O[2], h->O[3], h->tw[0], h->tw[1], h->tw[2], h->kax[0],
                     h->kax[1], h->kax[2], h->vdd, h->prms, h->sc, h->partials, h->stage128, h->Lo[0], h->Lo[1],
-                    h->k2s[0], h->k2s[1], h->k2s[2]};
+                    h->k2s[0], h->k2s[1], h->k2s[2], h->obs_part};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     void* cptrs[] = {h->ctrlG, h->V0, h->adj[0], h->adj[1], h->adj[2], h->adj[3], h->adj[4], h->adj[5], h->adj[6],
@@ -1325,6 +1375,63 @@ gpe_status gpe_momentum_x(gpe_handle* h, int comp, double* px) {
     GPE_TRY(sync_read_scalars(h, &s));
     *px = s.obs[1];
     return GPE_OK;
+}
+
+}  // extern "C"
+
+// kind: OBS_*; c2 < 0 for the one-field kinds.  Returns the sum times DV,
+// as the reference's reduction (src/baseHamiltonian.cu:112-150) does.
+template <typename R>
+gpe_status observable_t(gpe_handle* h, int kind, int c1, int c2, double sign, double* out) {
+    typedef typename Cx<R>::T C;
+    GPE_TRY(canonicalize_t<R>(h));
+    if (!h->obs_part) GPE_CUDA(cudaMalloc(&h->obs_part, sizeof(double) * (OBS_BLOCKS + 1)));
+    k_obs_partials<C><<<OBS_BLOCKS, 256, 0, h->st>>>(kind, (const C*)h->A[c1], c2 >= 0 ? (const C*)h->A[c2] : nullptr,
+                                                     sign, h->cfg.xmax[0], h->cfg.dx[0], 2.0 * h->cfg.xmax[0], h->nx,
+                                                     h->N, h->obs_part);
+    k_ctrl_final<<<1, 64, 0, h->st>>>(h->obs_part, OBS_BLOCKS, 1, h->obs_part + OBS_BLOCKS);
+    h->launches += 2;
+    GPE_CUDA(cudaGetLastError());
+    double r = 0.0;
+    GPE_CUDA(cudaMemcpyAsync(&r, h->obs_part + OBS_BLOCKS, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    GPE_CUDA(cudaStreamSynchronize(h->st));
+    *out = r * h->cfg.dx[0] * h->cfg.dx[1] * h->cfg.dx[2];
+    return GPE_OK;
+}
+
+gpe_status observable(gpe_handle* h, int kind, int c1, int c2, double sign, double* out) {
+    GPE_TRY(check_handle(h));
+    if (!out) return fail(GPE_ERR_INVALID_ARG, "null output");
+    if (h->nb != 1) return fail(GPE_ERR_INVALID_ARG, "observables of batched instances are not supported");
+    return h->prec == GPE_C64 ? observable_t<float>(h, kind, c1, c2, sign, out)
+                              : observable_t<double>(h, kind, c1, c2, sign, out);
+}
+
+extern "C" {
+
+gpe_status gpe_average_cos(gpe_handle* h, int comp, double* out) {
+    GPE_TRY(check_handle(h));
+    GPE_TRY(check_comp(h, comp));
+    return observable(h, OBS_COS, comp, -1, 0.0, out);
+}
+
+gpe_status gpe_average_cos2(gpe_handle* h, int sign, double* out) {
+    GPE_TRY(check_handle(h));
+    if (h->ncomp != 2) return fail(GPE_ERR_INVALID_ARG, "needs two components");
+    if (sign != 1 && sign != -1) return fail(GPE_ERR_INVALID_ARG, "sign must be +1 or -1");
+    return observable(h, OBS_COS2, 0, 1, (double)sign, out);
+}
+
+gpe_status gpe_relative_phase(gpe_handle* h, double* out) {
+    GPE_TRY(check_handle(h));
+    if (h->ncomp != 2) return fail(GPE_ERR_INVALID_ARG, "needs two components");
+    return observable(h, OBS_PHASE, 0, 1, 0.0, out);
+}
+
+gpe_status gpe_dsz_dt(gpe_handle* h, double* out) {
+    GPE_TRY(check_handle(h));
+    if (h->ncomp != 2) return fail(GPE_ERR_INVALID_ARG, "needs two components");
+    return observable(h, OBS_DSZ, 0, 1, 0.0, out);
 }
 
 gpe_status gpe_fft(gpe_handle* h, int comp, int sign) {

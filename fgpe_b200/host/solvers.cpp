@@ -62,13 +62,6 @@ void fill_grid(gpe_config& c, const ParamsBase& p) {
 }
 
 // <cos(2 pi x / L)>: CalcAverageCos, src/parallel.cu:535-561, times DV.
-double average_cos(const ParamsBase& p, const std::vector<complex>& psi) {
-    const double L = 2 * p.XMAX[0];
-    double s = 0.0;
-    for (int i = 0; i < p.Npoints; ++i) s += std::cos(2 * pi * gridX(p, i) / L) * std::norm(psi[i]);
-    return s * p.DV;
-}
-
 // First iteration i >= it (at most last) for which pred(i) holds.
 template <class Pred>
 int next_event(int it, int last, Pred pred) {
@@ -311,7 +304,7 @@ void BEConeComponent::call_RE_init() {
     PARS[EN_0] = o[2] / PARS[NORM];
     PARS[NORM] = o[0];
     if (!is_template) {
-        PARS[AUX1] = average_cos(p, psi);
+        chk(gpe_average_cos(h, 0, &PARS[AUX1]), "gpe_average_cos");  // alg_calcCos on the device
         PARS[AUX1] /= PARS[NORM];
     }
     PARS[PX] = calcPx();
@@ -331,8 +324,7 @@ void BEConeComponent::call_RE_loop_after_step() {
         PARS[MU] = last_obs[1] / PARS[NORM];
         PARS[EN] = last_obs[2] / PARS[NORM];
         if (!is_template) {
-            download_psi();
-            PARS[AUX1] = average_cos(p, psi);
+            chk(gpe_average_cos(h, 0, &PARS[AUX1]), "gpe_average_cos");
             PARS[AUX1] /= PARS[NORM];
         }
         PARS[PX] = calcPx();
@@ -601,8 +593,11 @@ void BECtwoComponent::call_RE_init() {
     PARS[EN2_0] = o[5] / PARS[NORM2];
     PARS[NORM1] = o[0];
     PARS[NORM2] = o[3];
-    PARS[AUX1_1] = average_cos(p, psi1) / PARS[NORM1];
-    PARS[AUX1_2] = average_cos(p, psi2) / PARS[NORM2];
+    double c1 = 0.0, c2 = 0.0;
+    chk(gpe_average_cos(h, 0, &c1), "gpe_average_cos");
+    chk(gpe_average_cos(h, 1, &c2), "gpe_average_cos");
+    PARS[AUX1_1] = c1 / PARS[NORM1];
+    PARS[AUX1_2] = c2 / PARS[NORM2];
     PARS[PX1] = calcPx(0) / ((PARS[NORM1] * hbar) / p.aho1);
     PARS[PX2] = calcPx(1) / ((PARS[NORM2] * hbar) / p.aho1);
     status_line_real(0.0);
@@ -620,9 +615,11 @@ void BECtwoComponent::call_RE_loop_after_step() {
         PARS[EN1] = o[2] / PARS[NORM1];
         PARS[MU2] = o[4] / PARS[NORM2];
         PARS[EN2] = o[5] / PARS[NORM2];
-        download_psi();
-        PARS[AUX1_1] = average_cos(p, psi1) / PARS[NORM1];
-        PARS[AUX1_2] = average_cos(p, psi2) / PARS[NORM2];
+        double c1 = 0.0, c2 = 0.0;
+        chk(gpe_average_cos(h, 0, &c1), "gpe_average_cos");
+        chk(gpe_average_cos(h, 1, &c2), "gpe_average_cos");
+        PARS[AUX1_1] = c1 / PARS[NORM1];
+        PARS[AUX1_2] = c2 / PARS[NORM2];
         PARS[PX1] = calcPx(0) / ((PARS[NORM1] * hbar) / p.aho1);
         PARS[PX2] = calcPx(1) / ((PARS[NORM2] * hbar) / p.aho1);
         status_line_real(p.time0 + PARS[ITER] * p.dt);

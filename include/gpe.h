@@ -195,6 +195,28 @@ gpe_status gpe_observables(gpe_handle* h, double t, double* out);
  * plugin's division: sum Re(conj(psi) IFFT(kx FFT psi)) DV with the
  * unnormalised inverse transform of the reference (kx in cycles/length). */
 gpe_status gpe_momentum_x(gpe_handle* h, int comp, double* px);
+
+/* Logging-cadence observables of the plugins' status lines, reduced on the
+ * device (FP64, compensated) and returned as the reference's reduction
+ * returns them: the grid sum times DV (src/baseHamiltonian.cu:112-150).
+ * x[ix] = -xmax[0] + (ix + 1/2) dx[0], L = 2 xmax[0].
+ * gpe_average_cos: sum cos(2 pi x/L) |psi_comp|^2 DV — alg_calcCos
+ *   (hamiltonians/BEC_oneComponent.cu:115-121, BEC_twoComponent.cu:147-152)
+ *   with CalcAverageCos (src/parallel.cu:535-561); the plugins divide it by
+ *   the norm (BEC_oneComponent.cu:349-350).
+ * gpe_average_cos2: the same for psi_0 + sign psi_1, sign = +1 or -1
+ *   (src/parallel.cu:739-771; the reference's two-field alg_calcCos,
+ *   BEC_twoComponent.cu:154-160, launches it without its sign, i.e. +1).
+ * gpe_relative_phase: sum (atan2 psi_0 - atan2 psi_1) DV
+ *   (CalculateRelativePhase, src/parallel.cu:774-802).
+ * gpe_dsz_dt: sum sqrt(|psi_0|^2 |psi_1|^2) sin(atan2 psi_0 - atan2 psi_1) DV
+ *   (CalculateDszDt, src/parallel.cu:805-839).
+ * The two-field forms need ncomp = 2.  A complex64 handle reduces the high
+ * part of its state. */
+gpe_status gpe_average_cos(gpe_handle* h, int comp, double* out);
+gpe_status gpe_average_cos2(gpe_handle* h, int sign, double* out);
+gpe_status gpe_relative_phase(gpe_handle* h, double* out);
+gpe_status gpe_dsz_dt(gpe_handle* h, double* out);
 /* Unnormalised 3D DFT of psi_comp in place, sign -1 (CUFFT_FORWARD) or +1
  * (CUFFT_INVERSE): the cufftExecZ2Z calls of src/baseHamiltonian.cu:89,95. */
 gpe_status gpe_fft(gpe_handle* h, int comp, int sign);

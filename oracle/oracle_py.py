@@ -87,6 +87,43 @@ def axes(cfg):
     return out
 
 
+# ---- logging-cadence observables: numpy restatements -----------------------------
+# x[ix] = -XMAX + (ix + 1/2) DX (src/baseHamiltonian.cu:25-51), L = 2 XMAX[0];
+# each returns the grid sum times DV, as the reference's reduction does
+# (src/baseHamiltonian.cu:112-150).  psi arrays are (nz, ny, nx).
+PI_REF = 3.141592653589793  # hpp/header.hpp:28
+
+
+def _cos_weight(cfg):
+    x = -cfg.xmax[0] + (np.arange(cfg.nx, dtype=np.float64) + 0.5) * cfg.dx[0]
+    return np.cos(2 * PI_REF * x / (2 * cfg.xmax[0]))
+
+
+def _dv(cfg):
+    return cfg.dx[0] * cfg.dx[1] * cfg.dx[2]
+
+
+def average_cos(cfg, psi):
+    """CalcAverageCos (src/parallel.cu:535-561): sum cos(2 pi x/L) |psi|^2 DV."""
+    return float(np.sum(_cos_weight(cfg) * np.abs(psi) ** 2) * _dv(cfg))
+
+
+def average_cos2(cfg, psi1, psi2, sign):
+    """CalcAverageCos for psi1 + sign psi2 (src/parallel.cu:739-771)."""
+    return float(np.sum(_cos_weight(cfg) * np.abs(psi1 + sign * psi2) ** 2) * _dv(cfg))
+
+
+def relative_phase_terms(psi1, psi2):
+    """CalculateRelativePhase (src/parallel.cu:774-802), per point."""
+    return np.arctan2(psi1.imag, psi1.real) - np.arctan2(psi2.imag, psi2.real)
+
+
+def dsz_dt_terms(psi1, psi2):
+    """CalculateDszDt (src/parallel.cu:805-839), per point."""
+    ph = relative_phase_terms(psi1, psi2)
+    return np.sqrt(np.abs(psi1) ** 2 * np.abs(psi2) ** 2) * np.sin(ph)
+
+
 class OracleSolver:
     """Same methods as fgpe_b200.Solver, computed on the host in FP64."""
 

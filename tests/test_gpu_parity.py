@@ -132,6 +132,32 @@ def test_real_time_call_splitting(gpu, prec, shape):
     assert rel(p1, o.get_psi(0)) < tol
 
 
+@pytest.mark.parametrize("prec", [C128, C64])
+def test_logging_observables(gpu, prec):
+    # The plugins' status-line reductions on the device against the numpy
+    # restatements of the reference kernels, on the state the device holds.
+    cfg = make_config((16, 12, 8), (5.0, 4.0, 3.0), precision=prec, hamiltonian=HAM_TEMPLATE)
+    g, _ = pair(cfg)
+    p = g.get_psi(0)
+    tol = TOL[prec]
+    want = orc.average_cos(cfg, p)
+    assert abs(g.average_cos(0) - want) <= tol * abs(want)
+    cfg2 = make_config((16, 12, 8), (5.0, 4.0, 3.0), precision=prec, ncomp=2, hamiltonian=HAM_BEC2,
+                       prms=[1.0, 1.0, 0.5], npart=(0.5, 0.5))
+    g2, _ = pair(cfg2)
+    p1, p2 = g2.get_psi(0), g2.get_psi(1)
+    dv = cfg2.dx[0] * cfg2.dx[1] * cfg2.dx[2]
+    for sign in (1, -1):
+        want = orc.average_cos2(cfg2, p1, p2, sign)
+        assert abs(g2.average_cos2(sign) - want) <= tol * abs(want)
+    for got, terms in ((g2.relative_phase(), orc.relative_phase_terms(p1, p2)),
+                       (g2.dsz_dt(), orc.dsz_dt_terms(p1, p2))):
+        # relative to the sum of magnitudes: the signed sums cancel
+        assert abs(got - np.sum(terms) * dv) <= tol * np.sum(np.abs(terms)) * dv
+    with pytest.raises(Exception):
+        g.relative_phase()  # one component
+
+
 def test_complex64_compensated_state(gpu):
     # complex64 carries the real-time step state as float32 high + low parts
     # (an error-free TwoSum at stage 4), across calls.  Rounding the state to
