@@ -96,6 +96,9 @@ public:
     double aho = 0, omho = 0, mass = 0, npart = 0, a = 0, add = 0, edd = 0;
     Params() = default;
     explicit Params(const InputVariables& iv);
+    // Params::RedefineLatticeSoft (src/params.cu:35-131), applied for
+    // hamiltonian "soft" before DX is derived from XMAX.
+    void redefine_lattice_soft();
     const double* _omega(int) const override { return omega; }
     const double* _ax(int) const override { return ax; }
     double _aho(int) const override { return aho; }

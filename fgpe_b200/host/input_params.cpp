@@ -96,6 +96,38 @@ bool InputVariables::getBool(const std::string& n) const {
     return it->second;
 }
 
+// Params::RedefineLatticeSoft, src/params.cu:35-131: for a soft-core droplet
+// lattice the domain is made a whole number of inter-droplet distances
+// idd = a_soft / (akrot / 2 pi) along each used axis, the distance scaled
+// per lattice type (triangular / HEX: y by sqrt(3); BCC: sqrt(2); SC:
+// 1/sqrt(2); FCC: sqrt(3)).  A missing akrot, a_soft or Latticetype key is
+// an error, as in the reference (whose getDouble / getString exit before its
+// try block could catch anything).  The BCC half-cell shift of the
+// reference (lines 111-115) is overwritten by the plain assignment that
+// follows it there, so it has no effect and is not repeated here.
+void Params::redefine_lattice_soft() {
+    {
+        const double akrot = iv.getDouble("akrot") / (2 * pi);
+        const double a = iv.getDouble("a_soft");
+        const double idd = a / akrot;
+        const double triangular = 2 * std::sqrt(3.) / 2.;
+        double dist[3] = {idd, idd, idd};
+        const std::string type = iv.getString("Latticetype");
+        if (type == "triangular" || type == "HEX") dist[1] = idd * triangular;
+        double f = 1.0;
+        bool all = false;
+        if (type == "BCC") { f = std::sqrt(2); all = true; }
+        if (type == "SC") { all = true; }
+        if (type == "FCC") { f = std::sqrt(3); all = true; }
+        if (all)
+            for (double& d : dist) d = (type == "SC") ? idd / std::sqrt(2) : idd * f;
+        for (int i = 0; i < DIM && i < 3; ++i) {
+            const int n = (int)std::round(2 * XMAX[i] / dist[i]);
+            XMAX[i] = 0.5 * n * dist[i];
+        }
+    }
+}
+
 // Params::InitializeParams, src/params.cu:134-219.
 Params::Params(const InputVariables& in) {
     iv = in;
@@ -114,8 +146,7 @@ Params::Params(const InputVariables& in) {
     XMAX[0] = iv.getDouble("xmax");
     XMAX[1] = iv.getDouble("ymax");
     XMAX[2] = iv.getDouble("zmax");
-    if (iv.has("hamiltonian") && iv.getVariable("hamiltonian") == "\"soft\"")
-        throw HostError("hamiltonian \"soft\" (soft-core lattice redefinition) is not supported");
+    if (iv.has("hamiltonian") && iv.getString("hamiltonian") == "soft") redefine_lattice_soft();
     for (int i = 0; i < 3; ++i) DX[i] = 2 * XMAX[i] / NX[i];
     omega[0] = 2 * pi * iv.getDouble("omx");
     omega[1] = 2 * pi * iv.getDouble("omy");
