@@ -28,7 +28,7 @@ LIB_PATH = os.path.join(HERE, "libgpe.so")
 
 NO_HAMIL_PARAMS = 32
 C128, C64 = 0, 1
-HAM_BEC, HAM_BEC2, HAM_TEMPLATE, HAM_DIPOLAR = 0, 1, 2, 3
+HAM_BEC, HAM_BEC2, HAM_TEMPLATE, HAM_DIPOLAR, HAM_SOFT = 0, 1, 2, 3, 4
 IMAG_HEAVYBALL, IMAG_RK4 = 0, 1
 ABI_VERSION = 1
 

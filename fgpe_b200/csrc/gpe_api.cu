@@ -285,6 +285,29 @@ __global__ void k_ctrl_final(const double* part, int nblocks, int nv, double* ou
 void host_vdd(const gpe_config& c, const std::vector<double>* k, std::vector<double>& out) {
     const long long N = (long long)c.nx * c.ny * c.nz;
     out.assign(N, 0.0);
+    if (c.hamiltonian == GPE_HAM_SOFT) {
+        // SoftCoreInteraction_1D/2D/3D, src/parallel.cu:360-477 (a = prms[0],
+        // U = prms[1], k = 2 pi |k|, small-k forms below 1e-6), / N
+        const double a = c.prms[0], U = c.prms[1], pi = 3.141592653589793;
+        for (int iz = 0; iz < c.nz; ++iz)
+            for (int iy = 0; iy < c.ny; ++iy)
+                for (int ix = 0; ix < c.nx; ++ix) {
+                    const long long idx = ((long long)iz * c.ny + iy) * c.nx + ix;
+                    const double kx = k[0][ix], ky = k[1][iy], kz = k[2][iz];
+                    const double kk = 2 * pi * std::sqrt(kx * kx + ky * ky + kz * kz);
+                    double v;
+                    if (c.dim == 1)
+                        v = kk < 1e-6 ? U * 2 * a * (1 - (a * kk) * (a * kk) / 6.0) : U * 2 * std::sin(a * kk) / kk;
+                    else if (c.dim == 2)
+                        v = kk < 1e-6 ? U * pi * a * a : 2 * pi * a * U * std::cyl_bessel_j(1.0, kk * a) / kk;
+                    else
+                        v = kk < 1e-6 ? U * (4. / 3.) * pi * std::pow(a, 3)
+                                      : 4 * pi * U * std::pow(a, 3) * (std::sin(kk * a) - kk * a * std::cos(kk * a)) /
+                                            std::pow(kk * a, 3);
+                    out[idx] = v / (double)N;
+                }
+        return;
+    }
     const double add = c.prms[6];
     double d[3] = {c.prms[7], c.prms[8], c.prms[9]};
     const double dn = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
@@ -1066,7 +1089,7 @@ gpe_status create_handle(const gpe_config* cfg, int nb, gpe_handle** out) {
     if (cfg->nx < 1 || cfg->ny < 1 || cfg->nz < 1) return fail(GPE_ERR_INVALID_ARG, "grid sizes must be >= 1");
     if (cfg->ncomp < 1 || cfg->ncomp > 2) return fail(GPE_ERR_INVALID_ARG, "ncomp must be 1 or 2");
     if (cfg->precision != GPE_C128 && cfg->precision != GPE_C64) return fail(GPE_ERR_INVALID_ARG, "bad precision");
-    if (cfg->hamiltonian < GPE_HAM_BEC || cfg->hamiltonian > GPE_HAM_DIPOLAR)
+    if (cfg->hamiltonian < GPE_HAM_BEC || cfg->hamiltonian > GPE_HAM_SOFT)
         return fail(GPE_ERR_INVALID_ARG, "bad hamiltonian");
     if (cfg->ncomp == 2 && cfg->hamiltonian != GPE_HAM_BEC2 && cfg->hamiltonian != GPE_HAM_TEMPLATE)
         return fail(GPE_ERR_UNSUPPORTED, "two components need GPE_HAM_BEC2 or GPE_HAM_TEMPLATE");
@@ -1089,7 +1112,7 @@ gpe_status create_handle(const gpe_config* cfg, int nb, gpe_handle** out) {
     h->nz = cfg->nz;
     h->N = (long long)cfg->nx * cfg->ny * cfg->nz;
     h->ncomp = cfg->ncomp;
-    h->dens = cfg->hamiltonian == GPE_HAM_DIPOLAR ? 1 : 0;
+    h->dens = (cfg->hamiltonian == GPE_HAM_DIPOLAR || cfg->hamiltonian == GPE_HAM_SOFT) ? 1 : 0;
     h->nf = h->ncomp + h->dens;
     h->esz = h->prec == GPE_C128 ? 16 : 8;
     h->nb = nb;

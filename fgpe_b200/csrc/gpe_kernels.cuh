@@ -211,7 +211,7 @@ struct HamCoef {
 template <typename R, typename C, int MC = 2>
 __device__ __forceinline__ void ham_point(int ham, int ncomp, const HamCoef<R>& hc, const C* psi, const C* T,
                                           const C* V, R phi, bool want_en, C* hmu, C* hen) {
-    if (ham == GPE_HAM_BEC || ham == GPE_HAM_DIPOLAR) {
+    if (ham == GPE_HAM_BEC || ham == GPE_HAM_DIPOLAR || ham == GPE_HAM_SOFT) {  // SOFT: g = 0
         const R px = psi[0].x, py = psi[0].y;
         const R n = px * px + py * py;
         R rX, rY;

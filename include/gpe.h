@@ -75,6 +75,15 @@ typedef enum gpe_precision { GPE_C128 = 0, GPE_C64 = 1 } gpe_precision;
  *                   is 12*pi*a_dd*((k.d)^2/k^2 - 1/3) as in
  *                   src/parallel.cu:326-352 (never called there), times
  *                   1 + 3cos(kR)/(kR)^2 - 3sin(kR)/(kR)^3 with k in rad/length.
+ *  GPE_HAM_SOFT     one component, h = T + (V + Phi) psi with the mean field
+ *                   Phi = IFFT(V~(k) FFT|psi|^2) / N of a soft-core
+ *                   interaction, V~ of SoftCoreInteraction_1D/2D/3D
+ *                   (src/parallel.cu:360-477, never called there) by
+ *                   gpe_config.dim: prms[0] = a (radius), prms[1] = U,
+ *                   k = 2 pi |k| in rad/length; 1D 2U sin(ak)/k, 2D
+ *                   2 pi a U J1(ka)/k, 3D 4 pi U a^3 (sin ka - ka cos ka)/(ka)^3,
+ *                   with the reference's small-k forms below k = 1e-6.  No
+ *                   contact term; the energy density takes Phi/2.
  *  Moving-frame term (the plugins' trotate option, BaseHamiltonian::alg_addVPx,
  *  src/baseHamiltonian.cu:198-211): for every Hamiltonian but the template,
  *  prms[11 + c] = lambda_c (2 pi omega / (omho aho) in the reference,
@@ -86,7 +95,8 @@ typedef enum gpe_hamiltonian {
     GPE_HAM_BEC = 0,
     GPE_HAM_BEC2 = 1,
     GPE_HAM_TEMPLATE = 2,
-    GPE_HAM_DIPOLAR = 3
+    GPE_HAM_DIPOLAR = 3,
+    GPE_HAM_SOFT = 4
 } gpe_hamiltonian;
 
 /* Imaginary-time scheme.

@@ -263,6 +263,10 @@ struct orc_solver {
     // (0 for |k| < 1e-6 as there), times the spherical cut-off factor
     // 1 + 3cos(q)/q^2 - 3sin(q)/q^3, q = 2 pi |k| R (its q -> 0 limit is 0).
     void build_vdd() {
+        if (cfg.hamiltonian == GPE_HAM_SOFT) {
+            build_vsoft();
+            return;
+        }
         if (cfg.hamiltonian != GPE_HAM_DIPOLAR) return;
         vdd.assign(N, 0.0);
         const double add = cfg.prms[6];
@@ -284,6 +288,32 @@ struct orc_solver {
                             double q = 2.0 * PI_REF * den * R;
                             v *= 1.0 + 3.0 * std::cos(q) / (q * q) - 3.0 * std::sin(q) / (q * q * q);
                         }
+                    }
+                    vdd[idx] = v;
+                }
+    }
+
+    // Soft-core kernel by dimension: SoftCoreInteraction_1D (src/parallel.cu:371-398),
+    // _2D (:412-439), _3D (:453-477); a = prms[0], U = prms[1], k = 2 pi |k|.
+    void build_vsoft() {
+        vdd.assign(N, 0.0);
+        const double a = cfg.prms[0], U = cfg.prms[1];
+        for (int iz = 0; iz < cfg.nz; ++iz)
+            for (int iy = 0; iy < cfg.ny; ++iy)
+                for (int ix = 0; ix < cfg.nx; ++ix) {
+                    long idx = ((long)iz * cfg.ny + iy) * cfg.nx + ix;
+                    double kx = k[0][ix], ky = k[1][iy], kz = k[2][iz];
+                    double kk = 2 * PI_REF * std::sqrt(kx * kx + ky * ky + kz * kz);
+                    double v;
+                    if (cfg.dim == 1) {
+                        if (kk < 1E-6) v = U * 2 * a * (1 - (a * kk) * (a * kk) / 6.0);
+                        else v = U * 2 * std::sin(a * kk) / (kk);
+                    } else if (cfg.dim == 2) {
+                        if (kk < 1E-6) v = U * PI_REF * a * a;
+                        else v = 2 * PI_REF * a * U * std::cyl_bessel_j(1.0, kk * a) / kk;
+                    } else {
+                        if (kk < 1E-6) v = U * (4. / 3.) * PI_REF * std::pow(a, 3);
+                        else v = 4 * PI_REF * U * std::pow(a, 3) * (std::sin(kk * a) - kk * a * std::cos(kk * a)) / (std::pow(kk * a, 3));
                     }
                     vdd[idx] = v;
                 }
@@ -362,10 +392,12 @@ struct orc_solver {
     void calc_hpsi(double t, bool want_en) {
         for (int c = 0; c < ncomp; ++c) laplace(psi[c].data(), hpsi[c].data());
         const int ham = cfg.hamiltonian;
-        if (ham == GPE_HAM_BEC || ham == GPE_HAM_DIPOLAR) {
-            const double a = quench_as(t, cfg.prms);
+        if (ham == GPE_HAM_BEC || ham == GPE_HAM_DIPOLAR || ham == GPE_HAM_SOFT) {
+            // soft core: no contact term, the mean field of the soft kernel
+            const double a = (ham == GPE_HAM_SOFT) ? 0.0 : quench_as(t, cfg.prms);
+            const bool field = ham == GPE_HAM_DIPOLAR || ham == GPE_HAM_SOFT;
             std::vector<cplx> phi;
-            if (ham == GPE_HAM_DIPOLAR) dipolar_field(psi[0].data(), phi);
+            if (field) dipolar_field(psi[0].data(), phi);
             const cplx* p = psi[0].data();
             const cplx* V = vext[0].data();
             cplx* hm = hpsi[0].data();
@@ -375,7 +407,7 @@ struct orc_solver {
                 const double px = p[i].real(), py = p[i].imag();
                 const double n = px * px + py * py;
                 const double Tx = hm[i].real(), Ty = hm[i].imag();
-                const double phid = (ham == GPE_HAM_DIPOLAR) ? phi[i].real() : 0.0;
+                const double phid = field ? phi[i].real() : 0.0;
                 double rX, rY;
                 if (want_en) {
                     rX = (V[i].real() + 2 * PI_REF * a * n) + 0.5 * phid;

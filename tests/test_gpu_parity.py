@@ -7,8 +7,8 @@ import numpy as np
 import pytest
 
 import oracle_py as orc
-from fgpe_b200 import (C64, C128, HAM_BEC, HAM_BEC2, HAM_DIPOLAR, HAM_TEMPLATE, IMAG_RK4, Solver, grid_axes,
-                       make_config)
+from fgpe_b200 import (C64, C128, HAM_BEC, HAM_BEC2, HAM_DIPOLAR, HAM_SOFT, HAM_TEMPLATE, IMAG_RK4, Solver,
+                       grid_axes, make_config)
 
 from test_oracle import PI_REF, gaussian, harmonic
 
@@ -280,6 +280,30 @@ def test_dipolar(gpu, prec):
         om, oe = o.apply_h(0.0, c_)
         assert rel(gm, om) < TOL[prec] * 2
         assert rel(ge, oe) < TOL[prec] * 2
+    tol = TOL[prec] if prec == C128 else 1e-5
+    g.step_imag(0, 10)
+    o.step_imag(0, 10)
+    assert rel(g.get_psi(0), o.get_psi(0)) < tol
+    g.step_real(0, 10)
+    o.step_real(0, 10)
+    assert rel(g.get_psi(0), o.get_psi(0)) < tol
+
+
+@pytest.mark.parametrize("prec", [C128, C64])
+@pytest.mark.parametrize("shape,box", [((64, 1, 1), (8.0, 1.0, 1.0)), ((24, 20, 1), (6.0, 5.0, 1.0)),
+                                       ((16, 16, 8), (6.0, 6.0, 3.0))])
+def test_soft_core(gpu, prec, shape, box):
+    # soft-core mean field (V~ of SoftCoreInteraction_1D/2D/3D by dimension)
+    prms = np.zeros(32)
+    prms[0] = 0.9   # a
+    prms[1] = 15.0  # U
+    cfg = make_config(shape, box, dt=1e-3, precision=prec, prms=prms, hamiltonian=HAM_SOFT, beta=0.5)
+    g, o = pair(cfg)
+    gm, ge = g.apply_h(0.0, 0)
+    om, oe = o.apply_h(0.0, 0)
+    assert rel(gm, om) < TOL[prec] * 2
+    assert rel(ge, oe) < TOL[prec] * 2
+    assert rel(g.observables(0.0), o.observables(0.0)) < TOL[prec] * 2
     tol = TOL[prec] if prec == C128 else 1e-5
     g.step_imag(0, 10)
     o.step_imag(0, 10)

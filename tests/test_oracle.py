@@ -216,3 +216,41 @@ def test_moving_frame_term_matches_numpy():
     want_en = T + (V.real + 2 * PI_REF * a * n + 1j * V.imag) * psi - 0.9 * P
     assert np.linalg.norm(hm - want_mu) <= 1e-13 * np.linalg.norm(want_mu)
     assert np.linalg.norm(he - want_en) <= 1e-13 * np.linalg.norm(want_en)
+
+
+@pytest.mark.parametrize("shape,box", [((32, 1, 1), (6.0, 1.0, 1.0)), ((16, 12, 1), (5.0, 4.0, 1.0)),
+                                       ((12, 10, 8), (5.0, 4.0, 3.5))])
+def test_soft_core_matches_numpy(shape, box):
+    # GPE_HAM_SOFT: h_mu = T + (V + Phi) psi, h_en = T + (V + Phi/2) psi, with
+    # Phi = ifftn(V~ fftn|psi|^2) and V~ the SoftCoreInteraction_1D/2D/3D
+    # formulas of src/parallel.cu:360-477 for the grid's dimension.
+    from scipy.special import j1
+    from fgpe_b200 import HAM_SOFT
+    prms = np.zeros(32)
+    prms[0], prms[1] = 0.8, 12.0
+    cfg = make_config(shape, box, dt=2e-3, prms=prms, hamiltonian=HAM_SOFT)
+    V = harmonic(cfg, (1.0, 1.3, 1.7))
+    psi = gaussian(cfg, noise=0.05)
+    s = orc.OracleSolver(cfg)
+    s.set_vext(0, V)
+    s.set_psi(0, psi)
+    hm, he = s.apply_h(0.0, 0)
+    kx, ky, kz = orc.axes(cfg)[3:]
+    K2 = kz[:, None, None] ** 2 + ky[None, :, None] ** 2 + kx[None, None, :] ** 2
+    N = psi.size
+    T = np.fft.ifftn(19.739208802 / N * K2 * np.fft.fftn(psi)) * N
+    a, U = prms[0], prms[1]
+    k = 2 * PI_REF * np.sqrt(K2)
+    ks = np.where(k < 1e-6, 1.0, k)
+    if cfg.dim == 1:
+        vt = np.where(k < 1e-6, U * 2 * a * (1 - (a * k) ** 2 / 6.0), U * 2 * np.sin(a * ks) / ks)
+    elif cfg.dim == 2:
+        vt = np.where(k < 1e-6, U * PI_REF * a * a, 2 * PI_REF * a * U * j1(ks * a) / ks)
+    else:
+        vt = np.where(k < 1e-6, U * 4.0 / 3.0 * PI_REF * a ** 3,
+                      4 * PI_REF * U * a ** 3 * (np.sin(ks * a) - ks * a * np.cos(ks * a)) / (ks * a) ** 3)
+    phi = np.fft.ifftn(vt * np.fft.fftn(np.abs(psi) ** 2)).real
+    want_mu = T + (V.real + phi + 1j * V.imag) * psi
+    want_en = T + (V.real + 0.5 * phi + 1j * V.imag) * psi
+    assert np.linalg.norm(hm - want_mu) <= 1e-12 * np.linalg.norm(want_mu)
+    assert np.linalg.norm(he - want_en) <= 1e-12 * np.linalg.norm(want_en)
