@@ -19,11 +19,16 @@
 #pragma once
 
 #include <complex>
+#include <condition_variable>
 #include <cstdio>
+#include <deque>
+#include <exception>
 #include <map>
+#include <mutex>
 #include <random>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/gpe.h"
@@ -185,6 +190,49 @@ private:
     FILE* status = nullptr;
 };
 
+// Asynchronous psi.wdat frame appends (frame_writer.cpp): push(suffixes)
+// queues the solver's current psi (all components) -- converted to
+// complex128 on the device and copied into one of two pinned host slots on
+// the default stream the solver's handle runs on -- and a writer thread
+// appends component c to <prefix><suffixes[c]>psi.wdat once the copy has
+// landed, so stepping continues while the files are written.  Frames reach
+// the files in push order; push() waits only when both slots are still being
+// written.  flush() returns when every queued frame is on disk and rethrows
+// a write error.
+class FrameWriter {
+public:
+    FrameWriter() = default;
+    FrameWriter(const FrameWriter&) = delete;
+    FrameWriter& operator=(const FrameWriter&) = delete;
+    ~FrameWriter();
+    bool started() const { return out_ != nullptr; }
+    void start(Output* out, gpe_handle* h, long long n, int ncomp);
+    void push(const std::vector<std::string>& suffixes);
+    void flush();
+
+private:
+    struct Frame {
+        int slot;
+        std::vector<std::string> suffixes;
+    };
+    void run();
+    Output* out_ = nullptr;
+    gpe_handle* h_ = nullptr;
+    long long n_ = 0;
+    int ncomp_ = 0;
+    void* dev_ = nullptr;
+    void* host_[2] = {nullptr, nullptr};
+    void* ev_[2] = {nullptr, nullptr};  // cudaEvent_t
+    bool busy_[2] = {false, false};
+    int slot_ = 0;
+    std::deque<Frame> queue_;
+    bool stop_ = false;
+    std::exception_ptr err_;
+    std::mutex m_;
+    std::condition_variable cv_;
+    std::thread thread_;
+};
+
 // ---- solver / plugin classes ------------------------------------------------------
 // Mirrors OneComponentGPSolver (src/oneComponentGPSolver.cu) over a libgpe handle.
 class OneComponentGPSolver {
@@ -216,12 +264,16 @@ public:
     virtual void call_RE_loop_after_step() {}
     virtual void call_RE_end() {}
     void download_psi();
+    // Appends the current psi to psi.wdat without stopping the stepping loop
+    // (a plugin's replacement for download_psi() + output.WritePsi(psi)).
+    void write_frame();
     int itStatMod() const;
     // raw norm / <psi|h_mu> / <psi|h_en> sums of the last status step
     double last_obs[6] = {0, 0, 0, 0, 0, 0};
 
 protected:
     gpe_config make_config(int hamiltonian) const;
+    FrameWriter frames;  // last member: destroyed (flushed) before output and h
 };
 
 class TwoComponentGPSolver {
@@ -247,8 +299,14 @@ public:
     virtual void call_RE_loop_after_step() {}
     virtual void call_RE_end() {}
     void download_psi();
+    // Appends psi1 and psi2 to <suffix1>psi.wdat and <suffix2>psi.wdat without
+    // stopping the stepping loop (replaces download_psi() + two WritePsi calls).
+    void write_frames(const std::string& suffix1, const std::string& suffix2);
     void upload();
     int itStatMod() const;
+
+protected:
+    FrameWriter frames;  // last member: destroyed (flushed) before output and h
 };
 
 // hamiltonians/BEC_oneComponent.{hpp,cu}

@@ -92,6 +92,10 @@ OneComponentGPSolver::OneComponentGPSolver(const Params& par, int hamiltonian) :
 }
 
 OneComponentGPSolver::~OneComponentGPSolver() {
+    try {
+        frames.flush();
+    } catch (...) {
+    }
     if (h) gpe_destroy(h);
 }
 
@@ -100,6 +104,11 @@ void OneComponentGPSolver::setHamiltonianParams(const double* prms) { chk(gpe_se
 int OneComponentGPSolver::itStatMod() const { return p.getInt("itStatMod"); }
 
 void OneComponentGPSolver::download_psi() { chk(gpe_get_psi(h, 0, (double*)psi.data()), "gpe_get_psi"); }
+
+void OneComponentGPSolver::write_frame() {
+    if (!frames.started()) frames.start(&output, h, p.Npoints, 1);
+    frames.push({""});
+}
 
 void OneComponentGPSolver::alg_calcHpsi(std::vector<complex>* hmu, std::vector<complex>* hen) {
     if (hmu) hmu->resize(p.Npoints);
@@ -141,6 +150,7 @@ void OneComponentGPSolver::runImagTimeEvol() {
         PARS[ITER] = nxt + 1;
         it = nxt + 1;
     }
+    frames.flush();
     download_psi();
     call_IM_end();
 }
@@ -170,6 +180,7 @@ void OneComponentGPSolver::runRealTimeEvol() {
         call_RE_loop_after_step();
         it = nxt + 1;
     }
+    frames.flush();
     download_psi();
     call_RE_end();
 }
@@ -255,10 +266,7 @@ void BEConeComponent::call_IM_loop_after_step() {
                  PARS[ITER_TIME], PARS[NORM], PARS[MU], PARS[EN], PARS[EN_PREV] - PARS[EN], PARS[PX] / hbar);
         output.WriteStatus(buf);
     }
-    if ((iteration + 1) % p.itmod == 0) {
-        download_psi();
-        output.WritePsi(psi.data(), p.Npoints);
-    }
+    if ((iteration + 1) % p.itmod == 0) write_frame();
 }
 
 void BEConeComponent::call_IM_loop_convergence() {
@@ -335,8 +343,7 @@ void BEConeComponent::call_RE_loop_after_step() {
         output.WriteStatus(buf);
     }
     if (((int)PARS[ITER] + 1) % p.itmod == 0) {
-        download_psi();
-        output.WritePsi(psi.data(), p.Npoints);
+        write_frame();
         PARS[NCYCLES]++;
     }
 }
@@ -372,7 +379,16 @@ TwoComponentGPSolver::TwoComponentGPSolver(const Params2& par) : p(par), output(
 }
 
 TwoComponentGPSolver::~TwoComponentGPSolver() {
+    try {
+        frames.flush();
+    } catch (...) {
+    }
     if (h) gpe_destroy(h);
+}
+
+void TwoComponentGPSolver::write_frames(const std::string& suffix1, const std::string& suffix2) {
+    if (!frames.started()) frames.start(&output, h, p.Npoints, 2);
+    frames.push({suffix1, suffix2});
 }
 
 int TwoComponentGPSolver::itStatMod() const { return p.getInt("itStatMod"); }
@@ -422,6 +438,7 @@ void TwoComponentGPSolver::runImagTimeEvol() {
         PARS[ITER] = nxt + 1;
         it = nxt + 1;
     }
+    frames.flush();
     download_psi();
     call_IM_end();
 }
@@ -448,6 +465,7 @@ void TwoComponentGPSolver::runRealTimeEvol() {
         PARS[ITER] = nxt + base + 1;
         it = nxt + 1;
     }
+    frames.flush();
     download_psi();
     call_RE_end();
 }
@@ -531,9 +549,7 @@ void BECtwoComponent::call_IM_loop_after_step() {
         status_line_imag();
     }
     if ((iteration + 1) % p.itmod == 0) {
-        download_psi();
-        output.WritePsi(psi1.data(), p.Npoints);
-        output.WritePsi(psi2.data(), p.Npoints);
+        write_frames("", "");  // both into psi.wdat, as hamiltonians/BEC_twoComponent.cu:316-317
         PARS[NCYCLES]++;
     }
 }
@@ -625,9 +641,7 @@ void BECtwoComponent::call_RE_loop_after_step() {
         status_line_real(p.time0 + PARS[ITER] * p.dt);
     }
     if (((int)PARS[ITER] + 1) % p.itmod == 0) {
-        download_psi();
-        output.WritePsi(psi1.data(), p.Npoints, "1");
-        output.WritePsi(psi2.data(), p.Npoints, "2");
+        write_frames("1", "2");
         PARS[NCYCLES]++;
     }
 }
