@@ -146,10 +146,27 @@ public:
     void initHarmonic(const ParamsBase& p, int type);
     void normalize(const ParamsBase& p, int type = -1);
     void imprintVortexTube(const ParamsBase& p, double Ncirc);
+    // Lattice seeds for soft-core droplet crystals (src/psi.cu:179-348): add
+    // amp * (a sum of plane-wave cosines of wave number k, offset by off*)
+    // times sqrt(npart / dV) to psi, then normalise to the first component's
+    // particle number (the reference always passes 1 there).
+    void force1DLattice(const ParamsBase& p, double amp, double k, double off, int type = 1);
+    void force2DTriangularLattice(const ParamsBase& p, double amp, double k, double offx, double offy, int type = 1);
+    void force2DSquareLattice(const ParamsBase& p, double amp, double k, double offx, double offy, int type = 1);
+    void force3DHEXLattice(const ParamsBase& p, double amp, double k, double offx, double offy, double offz,
+                           int type = 1);
+    void force3DFCCLattice(const ParamsBase& p, double amp, double k, double offx, double offy, double offz,
+                           int type = 1);
+    void force3DBCCLattice(const ParamsBase& p, double amp, double k, double offx, double offy, double offz,
+                           int type = 1);
+    void force3DSCLattice(const ParamsBase& p, double amp, double k, double offx, double offy, double offz,
+                          int type = 1);
     void readPsi(const std::string& prefix, int length);
     complex* getPsi() { return psi.data(); }
 
 private:
+    template <class Shape>
+    void add_lattice(const ParamsBase& p, int type, Shape shape);
     std::mt19937 generator;
     std::uniform_real_distribution<double> distribution{-1.0, 1.0};
     complex noise(double rrnd, double crnd);

@@ -101,6 +101,31 @@ int gpeh_init_psi(const char* file, int type, double* out) {
     }
 }
 
+int gpeh_init_psi_lattice(const char* file, int lattice, double amp, double k, double offx, double offy,
+                          double offz, int type, double* out) {
+    try {
+        gpe::InputVariables iv{std::string(file)};
+        gpe::Params p(iv);
+        gpe::Psi ps(p, std::string(""));
+        if (p.getBool("tpi_vortex")) ps.imprintVortexTube(p, p.getDouble("api_prc"));
+        switch (lattice) {
+            case 1: ps.force1DLattice(p, amp, k, offx, type); break;
+            case 2: ps.force2DTriangularLattice(p, amp, k, offx, offy, type); break;
+            case 3: ps.force2DSquareLattice(p, amp, k, offx, offy, type); break;
+            case 4: ps.force3DHEXLattice(p, amp, k, offx, offy, offz, type); break;
+            case 5: ps.force3DFCCLattice(p, amp, k, offx, offy, offz, type); break;
+            case 6: ps.force3DBCCLattice(p, amp, k, offx, offy, offz, type); break;
+            case 7: ps.force3DSCLattice(p, amp, k, offx, offy, offz, type); break;
+            default: throw gpe::HostError("unknown lattice " + std::to_string(lattice));
+        }
+        std::memcpy(out, ps.psi.data(), sizeof(gpe::complex) * p.Npoints);
+        return 0;
+    } catch (const std::exception& e) {
+        g_host_err = e.what();
+        return -1;
+    }
+}
+
 int gpeh_init_vext(const char* file, int type, double* out) {
     try {
         gpe::InputVariables iv{std::string(file)};

@@ -105,6 +105,84 @@ void Psi::imprintVortexTube(const ParamsBase& p, double Ncirc) {
     }
 }
 
+// ---- lattice seeds, src/psi.cu:179-348 ---------------------------------------------
+// shape(i) is the seed amplitude at point i; its cosine sums are grouped and
+// ordered as the reference groups them, so the result is the same to the bit.
+template <class Shape>
+void Psi::add_lattice(const ParamsBase& p, int type, Shape shape) {
+    const double npart = (type == 1) ? p._npart(1) : p._npart(2);
+    const double avg = std::pow(npart / (p.DX[0] * p.DX[1] * p.DX[2]), 0.5);
+    for (int i = 0; i < p.Npoints; ++i) psi[i] = shape(i) * avg + psi[i];
+    normalize(p, 1);
+}
+
+void Psi::force1DLattice(const ParamsBase& p, double amp, double k, double off, int type) {
+    add_lattice(p, type, [&](int i) {
+        const double x = gridX(p, i) - off;
+        return amp * (1 - std::cos(k * x)) / 2.;  // 0 .. amp
+    });
+}
+
+void Psi::force2DTriangularLattice(const ParamsBase& p, double amp, double k, double offx, double offy, int type) {
+    const double h = std::sqrt(3.0) / 2;  // sin 60 deg
+    add_lattice(p, type, [&](int i) {
+        const double x = gridX(p, i) - offx, y = gridY(p, i) - offy;
+        return amp * (std::cos(k * x) + std::cos(k * (-0.5 * x + h * y)) + std::cos(k * (-0.5 * x - h * y))) / 3;
+    });
+}
+
+void Psi::force2DSquareLattice(const ParamsBase& p, double amp, double k, double offx, double offy, int type) {
+    add_lattice(p, type, [&](int i) {
+        const double x = gridX(p, i) - offx, y = gridY(p, i) - offy;
+        return amp * (std::cos(k * y) + std::cos(k * x)) / 2;
+    });
+}
+
+void Psi::force3DHEXLattice(const ParamsBase& p, double amp, double k, double offx, double offy, double offz,
+                            int type) {
+    const double r3 = std::sqrt(3.);
+    add_lattice(p, type, [&](int i) {
+        const double x = gridX(p, i) - offx, y = gridY(p, i) - offy, z = gridZ(p, i) - offz;
+        const double u = (-x + r3 * y) / 2., w = (-x - r3 * y) / 2.;  // the in-plane directions at +-120 deg
+        return amp * (std::cos(k * u) + std::cos(k * x) + std::cos(k * z) + std::cos(k * w)) / 4.0;
+    });
+}
+
+void Psi::force3DFCCLattice(const ParamsBase& p, double amp, double k, double offx, double offy, double offz,
+                            int type) {
+    const double r3 = std::sqrt(3.);
+    add_lattice(p, type, [&](int i) {
+        const double x = gridX(p, i) - offx, y = gridY(p, i) - offy, z = gridZ(p, i) - offz;
+        // the nine projections of the reference, in its order
+        const double q[9] = {(x + y - z) / r3, (y + z - x) / r3, (z + x - y) / r3,
+                             (x - y - z) / r3, (y - z - x) / r3, (z - x - y) / r3,
+                             (x + y + z) / r3, (y + z + x) / r3, (z + x + y) / r3};
+        double s = std::cos(k * q[0]);
+        for (int j = 1; j < 9; ++j) s = s + std::cos(k * q[j]);
+        return amp * s / 9.0;
+    });
+}
+
+void Psi::force3DBCCLattice(const ParamsBase& p, double amp, double k, double offx, double offy, double offz,
+                            int type) {
+    const double r2 = std::sqrt(2.0);
+    add_lattice(p, type, [&](int i) {
+        const double x = gridX(p, i) - offx, y = gridY(p, i) - offy, z = gridZ(p, i) - offz;
+        const double q[6] = {(x + y) / r2, (z + y) / r2, (z + x) / r2, (x - y) / r2, (z - y) / r2, (z - x) / r2};
+        double s = std::cos(k * q[0]);
+        for (int j = 1; j < 6; ++j) s = s + std::cos(k * q[j]);
+        return amp * s / 6;
+    });
+}
+
+void Psi::force3DSCLattice(const ParamsBase& p, double amp, double k, double offx, double offy, double offz,
+                           int type) {
+    add_lattice(p, type, [&](int i) {
+        const double x = gridX(p, i) - offx, y = gridY(p, i) - offy, z = gridZ(p, i) - offz;
+        return amp * (std::cos(k * z) + std::cos(k * y) + std::cos(k * x)) / 3;
+    });
+}
+
 // src/psi.cu:378-395 (a missing or short file is an error here, not a read
 // from NULL).
 void Psi::readPsi(const std::string& prefix, int length) {

@@ -30,6 +30,14 @@ int         gpeh_init_psi(const char* input_file, int type, double* out_c128);
 /* Initial Vext of the BEC plugins (hamiltonians/BEC_oneComponent.cu:63-83,
  * hamiltonians/BEC_twoComponent.cu:80-110). */
 int         gpeh_init_vext(const char* input_file, int type, double* out_c128);
+/* The one-component initial psi of gpeh_init_psi with a lattice seed added
+ * (Psi::force*Lattice, src/psi.cu:179-348, used to start soft-core droplet
+ * crystals): lattice 1 = 1D (offset offx), 2 = 2D triangular, 3 = 2D square,
+ * 4 = 3D HEX, 5 = 3D FCC, 6 = 3D BCC, 7 = 3D simple cubic; amp, wave number k
+ * and offsets in code units; type selects the particle number of the seed
+ * (1 or 2).  Returns 0 or -1 (gpeh_last_error). */
+int         gpeh_init_psi_lattice(const char* input_file, int lattice, double amp, double k, double offx,
+                                  double offy, double offz, int type, double* out_c128);
 /* Output::WriteWtxt / WriteWtxt_2c + WriteVariable2WTXT lines under the input
  * file's outprefix (src/output.cu:26-191). */
 int         gpeh_write_info(const char* input_file, int ncycles, int nvars, const char** names,

@@ -92,6 +92,29 @@ int ref_init_psi(const char* file, int type, double* out) {
     return 0;
 }
 
+// The one-component Psi of ref_init_psi with one of the reference's lattice
+// seeds applied (src/psi.cu:179-348); lattice numbering as gpeh_init_psi_lattice.
+int ref_init_psi_lattice(const char* file, int lattice, double amp, double k, double offx, double offy,
+                         double offz, int type, double* out) {
+    InputVariables reader{std::string(file)};
+    Params p(reader);
+    Psi* ps = new Psi(p, std::string(""));
+    if (p.getBool("tpi_vortex")) ps->imprintVortexTube(p, p.getDouble("api_prc"));
+    switch (lattice) {
+        case 1: ps->force1DLattice(p, amp, k, offx, type); break;
+        case 2: ps->force2DTriangularLattice(p, amp, k, offx, offy, type); break;
+        case 3: ps->force2DSquareLattice(p, amp, k, offx, offy, type); break;
+        case 4: ps->force3DHEXLattice(p, amp, k, offx, offy, offz, type); break;
+        case 5: ps->force3DFCCLattice(p, amp, k, offx, offy, offz, type); break;
+        case 6: ps->force3DBCCLattice(p, amp, k, offx, offy, offz, type); break;
+        case 7: ps->force3DSCLattice(p, amp, k, offx, offy, offz, type); break;
+        default: delete ps; return -1;
+    }
+    std::memcpy(out, ps->getPsi(), sizeof(complex) * p.Npoints);
+    delete ps;
+    return 0;
+}
+
 // Vext of the plugins, hamiltonians/BEC_oneComponent.cu:63-83 and
 // hamiltonians/BEC_twoComponent.cu:80-110.
 int ref_init_vext(const char* file, int type, double* out) {

@@ -147,3 +147,30 @@ def test_input_typing_rules(tmp_path):
     out = np.zeros(47)
     assert ours().gpeh_params(str(fn).encode(), dp(out)) == 1
     assert out[22] == 1 and out[0] == 32
+
+
+@needs_ref
+@pytest.mark.parametrize("lattice", [1, 2, 3, 4, 5, 6, 7])
+@pytest.mark.parametrize("case", ["bec_harmonic_3d.txt", "bec_2d.txt"])
+def test_lattice_seed_bit_identical(case, lattice, tmp_path):
+    # Psi::force*Lattice seeds (1D, 2D triangular/square, 3D HEX/FCC/BCC/SC)
+    # added to the plugin's initial psi, against the reference's Psi class.
+    f = materialise(case, tmp_path)
+    p = np.zeros(47)
+    ours().gpeh_params(f, dp(p))
+    n = int(p[4])
+    a = np.zeros(n, np.complex128)
+    b = np.zeros(n, np.complex128)
+    args = (lattice, 0.7, 1.9, 0.3, -0.2, 0.1, 1)
+    L = ours()
+    R = ref()
+    D = ctypes.c_double
+    sig = [ctypes.c_char_p, ctypes.c_int, D, D, D, D, D, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    L.gpeh_init_psi_lattice.argtypes = sig
+    R.ref_init_psi_lattice.argtypes = sig
+    assert L.gpeh_init_psi_lattice(f, *args, dp(a.view(np.float64))) == 0
+    assert R.ref_init_psi_lattice(f, *args, dp(b.view(np.float64))) == 0
+    assert np.array_equal(a, b), np.max(np.abs(a - b))
+    base = np.zeros(n, np.complex128)
+    L.gpeh_init_psi(f, 0, dp(base.view(np.float64)))
+    assert not np.array_equal(a, base)  # the seed changed psi
