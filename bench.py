@@ -63,6 +63,7 @@ def parse():
                         "256^2 optimal-control problem (separate JSON lines)")
     p.add_argument("--fd-components", type=int, default=32, help="control2d: finite-difference checks")
     p.add_argument("--sweep-instances", type=int, default=256)
+    p.add_argument("--no-tune", action="store_true", help="keep the default pass variants (no autotuning)")
     p.add_argument("--sweep-converge", action="store_true",
                    help="sweep2d: also run every instance to |dmu| < 1e-8 and report the iterations")
     return p.parse_args()
@@ -101,6 +102,12 @@ def initial_psi(cfg, seed=1):
     psi = g * (1 + 1e-3 * (rng.standard_normal(g.shape) + 1j * rng.standard_normal(g.shape)))
     dv = cfg.dx[0] * cfg.dx[1] * cfg.dx[2]
     return psi / np.sqrt(np.sum(np.abs(psi) ** 2) * dv)
+
+
+def workload_conf(n, world=1):
+    """The `config` object both arms print (the same workload)."""
+    return {"workload": f"real-time RK4 quench, {n}^3 on [-10,10]^3, V=0.5(x^2+y^2+4z^2), g 1000->1100, dt 5e-4",
+            "grid": [n, n, n], "parallelism": "replicas" if world > 1 else "single GPU"}
 
 
 def ground_state(n, stream_ptr, iters=3000):
@@ -213,6 +220,14 @@ def run_ours(args):
     psi_gs, prep = ground_state(n, stream_ptr, args.ground_steps)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
+    # autotune the pass variants of both forms for this grid (setup, like a
+    # transform planner: outside the timed region), then create the handles
+    tune_cache = os.path.join("/tmp", f"gpe_tune_{os.getpid()}.jsonl")
+    tuning = {}
+    if not args.no_tune:
+        for name, prec in (("c64", gp.C64), ("c128", gp.C128)):
+            tuning[name] = gp.tune(workload_config(n, prec, G1), 0, tune_cache)
+        gp.set_tune_cache(tune_cache)
     solvers = {}
     for name, prec in (("c64", gp.C64), ("c128", gp.C128)):
         cfg = workload_config(n, prec, G1)
@@ -300,11 +315,9 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded Gaussian -> heavy-ball ground state at g=1000, quench to g=1100)",
-        "config": {"workload": f"real-time RK4 quench, {n}^3 on [-10,10]^3, V=0.5(x^2+y^2+4z^2), "
-                               f"g 1000->1100, dt 5e-4",
-                   "grid": [n, n, n], "form": "complex64 fields/FFT, FP64 stage coefficients and reductions",
-                   "l2": "flushed before every timed step (256 MiB write)",
-                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "config": workload_conf(n, world),
+        "form": "complex64 fields/FFT, FP64 stage coefficients and reductions",
+        "l2": "flushed before every timed step (256 MiB write)",
         "plain_c128": {"value": round(value128, 2), "unit": "steps/s", "ms_per_step": round(ms128 / K, 5),
                        "speedup_c64_over_c128": round(value / value128, 3)},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
@@ -317,6 +330,7 @@ def run_ours(args):
                      "per_kind_ms_per_launch": {k: round(v[0] / v[1], 5) for k, v in prof.items() if v[1]},
                      "profiled_ms_per_step": round(results["c64"]["ms_prof"] / K, 5)},
         "e2e": e2e,
+        "tuning": tuning or "off (--no-tune): default pass variants",
         "gpu_launches": results["c64"]["launches"],
         "clocks": clocks,
         "prep": prep,
@@ -324,7 +338,7 @@ def run_ours(args):
 
     if not args.quick:
         line["accuracy"] = accuracy(solvers, psi_gs, args.accuracy_steps)
-        line["cpu_baseline"] = cpu_baseline(n)
+        line["cpu_baseline"] = cpu_baseline(n, psi_gs, solvers)
     else:
         line["cpu_baseline"] = None
     for s2 in solvers.values():
@@ -361,8 +375,11 @@ def accuracy(solvers, psi_gs, nsteps):
     return out
 
 
-def cpu_baseline(n, budget_s=12.0):
-    """FP64 oracle port of the reference algorithm on the host cores."""
+def cpu_baseline(n, psi_gs, solvers=None, budget_s=12.0):
+    """FP64 oracle port of the reference algorithm on the host cores, timed
+    over a bounded sample of the workload: k RK4 steps from the same ground
+    state.  The oracle's state after the sample is then the checker for both
+    GPU forms run over the same k steps (psi, E and mu relative errors)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py as orc
     import fgpe_b200 as gp
@@ -371,27 +388,67 @@ def cpu_baseline(n, budget_s=12.0):
     cfg = workload_config(n, gp.C128, G1)
     o = orc.OracleSolver(cfg)
     o.set_vext(0, trap(cfg))
-    o.set_psi(0, initial_psi(cfg))
+    o.set_psi(0, psi_gs)
     t0 = time.perf_counter()
     o.step_real(0, 1)
     one = time.perf_counter() - t0
     k = max(1, int(budget_s / max(one, 1e-3)))
     t0 = time.perf_counter()
-    o.step_real(1, k)
+    oo = o.step_real(1, k, want_obs=True)
     dt = time.perf_counter() - t0
+    po = o.get_psi(0)
     o.close()
-    return {"value": round(k / dt, 4), "unit": "steps/s", "cores": threads, "kind": "port",
-            "sample": f"{k} RK4 steps of the same {n}^3 workload in FP64 (oracle/gpe_oracle.cpp, OpenMP)"}
+    out = {"value": round(k / dt, 4), "unit": "steps/s", "cores": threads, "kind": "port",
+           "sample": f"{k + 1} RK4 steps of the same {n}^3 workload from the same ground state in FP64 "
+                     f"(oracle/gpe_oracle.cpp, OpenMP); {k} of them timed"}
+    if solvers:
+        par = {"steps": k + 1}
+        for name, s in solvers.items():
+            s.set_psi(0, psi_gs)
+            og = s.step_real(0, k + 1, want_obs=True)
+            pg = s.get_psi(0)
+            par[name] = {"psi_rel_l2": float(np.linalg.norm(pg - po) / np.linalg.norm(po)),
+                         "E_rel_err": float(abs(og[2] / og[0] - oo[2] / oo[0]) / abs(oo[2] / oo[0])),
+                         "mu_rel_err": float(abs(og[1] / og[0] - oo[1] / oo[0]) / abs(oo[1] / oo[0])),
+                         "norm_rel_err": float(abs(og[0] / oo[0] - 1))}
+        out["parity_vs_port"] = par
+    return out
+
+
+def reference_cuda_build(n):
+    """The reference's own CUDA build (complex128, cuFFT; oracle/_ref, built
+    from its sources) timed on this GPU for the same real-time RK4 loop: a
+    comparison figure carried in the reference arm's line."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    try:
+        import tempfile
+        import time_ref_build as trb
+        if not os.path.exists(trb.BIN):
+            return {"unavailable": "oracle/_ref/gpe_ref_trace not built"}
+        n1, n2, rep = 200, 1200, 3
+        with tempfile.TemporaryDirectory() as work:
+            trb.run(n, 10, work)
+            diffs = sorted((trb.run(n, n2, work) - trb.run(n, n1, work)) / (n2 - n1) for _ in range(rep))
+        per = diffs[len(diffs) // 2]
+        return {"steps_per_s": round(1.0 / per, 2), "ms_per_step": round(1e3 * per, 4), "dtype": "f64",
+                "method": f"median over {rep} of loop(niter={n2}) - loop(niter={n1}), device-synchronised wall "
+                          "time of the reference's own runRealTimeEvol loop"}
+    except Exception as e:  # comparison only: never fail the arm
+        return {"unavailable": str(e)[:200]}
 
 
 def run_reference(args):
-    """CPU reference arm: the oracle port (the reference has no CPU path)."""
+    """CPU reference arm: the FP64 oracle port of the reference's algorithm on
+    the host cores (the reference has no CPU path), same workload, warm-up and
+    config as the GPU arm.  Its line also carries the reference's own CUDA
+    build timed on this GPU (comparison only)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py as orc
     import fgpe_b200 as gp
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     threads = os.cpu_count() or 1
     orc.set_threads(threads)
     n = args.grid
@@ -399,28 +456,29 @@ def run_reference(args):
     o = orc.OracleSolver(cfg)
     o.set_vext(0, trap(cfg))
     o.set_psi(0, initial_psi(cfg))
-    W, K = max(args.warmup, 1), args.steps
-    # bounded sample: at most ~60 s of timed CPU work
+    W, K = max(args.warmup, 3), args.steps
     t0 = time.perf_counter()
     o.step_real(0, 1)
     one = time.perf_counter() - t0
+    o.step_real(1, W - 1)
+    # bounded sample: at most ~60 s of timed CPU work
     K = max(1, min(K, int(60.0 / max(one, 1e-3))))
-    W = min(W, 2)
-    o.step_real(1, W - 1) if W > 1 else None
     t0 = time.perf_counter()
     o.step_real(W, K)
     dt = time.perf_counter() - t0
     v = K / dt
     line = {"impl": "reference", "metric": "RK4 steps/s at 128^3 (complex64 + FP64 reductions, real-time quench)",
-            "value": round(v, 4), "unit": "steps/s", "n_gpus": 1, "steps": K, "warmup": W,
+            "value": round(v, 4), "unit": "steps/s", "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": round(1e3 * dt / K, 3), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"real-time RK4 quench, {n}^3 on [-10,10]^3, V=0.5(x^2+y^2+4z^2), "
-                                   f"g 1000->1100, dt 5e-4", "grid": [n, n, n]},
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian start)",
+            "config": workload_conf(n, world),
+            "form": "complex128 FP64 (oracle port of the reference's algorithm)",
             "cpu_baseline": {"value": round(v, 4), "unit": "steps/s", "cores": threads, "kind": "port",
-                             "sample": f"{K} FP64 RK4 steps (oracle port of the reference algorithm; "
-                                       f"the reference has no CPU path)"},
+                             "sample": f"{K} FP64 RK4 steps of the {n}^3 workload after {W} warm-up steps "
+                                       f"(oracle port of the reference algorithm; the reference has no CPU path)"},
             "e2e": {"value": round(v, 4), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    o.close()
+    line["reference_cuda_build"] = reference_cuda_build(n)
     print(json.dumps(line))
 
 
@@ -509,6 +567,9 @@ def run_sweep(args):
     stream = torch.cuda.Stream()
     b = gp.Batch([c for c, *_ in inst])
     b.set_stream(stream.cuda_stream)
+    # autotune every geometry group in place: per group the default and the
+    # tuned microseconds per iteration, measured on the same work
+    tune_rep = None if args.no_tune else b.tune(os.path.join("/tmp", f"gpe_tune_{os.getpid()}.jsonl"))
     for i, (c, V, p, *_ ) in enumerate(inst):
         b.set_vext(i, V)
         b.set_psi(i, p)
@@ -586,7 +647,9 @@ def run_sweep(args):
                          "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": round(alg_bytes / (ms / 1e3) / 1e9 / peak, 4), "traffic": None,
                          "model": "45 F per RK4 imaginary iteration, F = N*8 B"},
-            "gpu_launches": launches, "convergence": conv}
+            "tuning": tuning_summary(tune_rep, inst),
+            "gpu_launches": launches, "convergence": conv,
+            "cpu_baseline": sweep_cpu_leg(everything, stream)}
     if world > 1:
         line["n_gpus"] = world
         line["config"]["parallelism"] = "instances sharded over ranks by estimated cost (no data-path collective)"
@@ -594,6 +657,73 @@ def run_sweep(args):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def tuning_summary(rep, inst):
+    """Per-group autotuner result of the sweep: default and tuned iteration
+    times of each geometry group, and the sum over groups (one iteration of
+    every group, as the captured graph runs them)."""
+    if rep is None:
+        return "off (--no-tune): default pass variants"
+    sizes = []
+    for (c, *_rest) in inst:
+        key = (c.nx, c.ny)
+        if key not in sizes:
+            sizes.append(key)
+    groups = {f"{nx}x{ny}": {"default_us": round(d, 2), "tuned_us": round(t, 2)} for (nx, ny), (d, t) in
+              zip(sizes, rep)}
+    tot_d = sum(d for d, _ in rep)
+    tot_t = sum(t for _, t in rep)
+    return {"groups": groups, "iteration_default_us": round(tot_d, 2), "iteration_tuned_us": round(tot_t, 2),
+            "speedup": round(tot_d / tot_t, 3) if tot_t > 0 else None}
+
+
+def sweep_cpu_leg(everything, stream, k=20, sizes=(64, 192, 512)):
+    """CPU leg of the sweep: the FP64 oracle port timed on one seeded instance
+    of each of a few sizes for k RK4 imaginary-time iterations, and, as the
+    checker, those instances advanced together as one complex64 batch over
+    the same iterations (psi, E, mu relative errors)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as orc
+    import fgpe_b200 as gp
+    threads = os.cpu_count() or 1
+    orc.set_threads(threads)
+    picks = []
+    for want in sizes:
+        for i, item in enumerate(everything):
+            if item[3] == want:
+                picks.append(i)
+                break
+    b = gp.Batch([everything[i][0] for i in picks])
+    b.set_stream(stream.cuda_stream)
+    for j, i in enumerate(picks):
+        b.set_vext(j, everything[i][1])
+        b.set_psi(j, everything[i][2])
+    b.step_imag(k)
+    res, t_cpu, pts = {}, 0.0, 0
+    for j, i in enumerate(picks):
+        cfg, V, p, n, g, aniso = everything[i]
+        c128 = cfg.copy()
+        c128.precision = gp.C128
+        o = orc.OracleSolver(c128)
+        o.set_vext(0, V)
+        o.set_psi(0, p)
+        t0 = time.perf_counter()
+        o.step_imag(0, k)
+        t_cpu += time.perf_counter() - t0
+        pts += k
+        so, po = o.imag_state(), o.get_psi(0)
+        o.close()
+        sb, pb = b.imag_state(j), b.get_psi(j)
+        res[f"instance_{i}_N{n}"] = {"g": round(g, 3), "aniso": round(aniso, 4),
+                                     "psi_rel_l2": float(np.linalg.norm(pb - po) / np.linalg.norm(po)),
+                                     "E_rel_err": float(abs(sb[2] / so[2] - 1)),
+                                     "mu_rel_err": float(abs(sb[1] / so[1] - 1))}
+    b.close()
+    return {"value": round(pts / t_cpu, 3), "unit": "instance-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{k} RK4 imaginary-time iterations of {len(picks)} seeded instances (N = {list(sizes)}) in "
+                      f"FP64 (oracle/gpe_oracle.cpp)",
+            "parity_vs_port": {"iterations": k, "form": "complex64 batch", "instances": res}}
 
 
 def control_problem(precision, nsteps=2000, n=256, seed=5):
@@ -755,10 +885,14 @@ def run_imag(args):
     out = {"metric": "imaginary-time iterations/s", "unit": "iterations/s", "n_gpus": 1, "cases": {}}
     forms = [("c128_heavyball", gp.C128, gp.IMAG_HEAVYBALL), ("c128_rk4", gp.C128, gp.IMAG_RK4),
              ("c64_rk4", gp.C64, gp.IMAG_RK4)]
+    cache = os.path.join("/tmp", f"gpe_tune_{os.getpid()}.jsonl")
+    if not args.no_tune:
+        gp.set_tune_cache(cache)
     for name in ("ground64", "dipolar", "twocomp"):
         res = {}
         for form, prec, scheme in forms:
             cfg, V, psis = imag_case(name, prec, scheme)
+            tuned = None if args.no_tune else gp.tune(cfg, 1, cache)
             s = gp.Solver(cfg)
             s.set_stream(st.cuda_stream)
             for c in range(cfg.ncomp):
@@ -779,11 +913,66 @@ def run_imag(args):
                 total += d
             st8 = s.imag_state()
             res[form] = {"iterations_per_s": round(ips, 1), "converged": bool(conv), "iterations": int(total),
+                         "tuning": tuned,
                          "mu": [float(st8[4 * c + 1]) for c in range(cfg.ncomp)],
                          "E": [float(st8[4 * c + 2]) for c in range(cfg.ncomp)]}
             s.close()
+        for form in ("c128_rk4", "c64_rk4"):
+            if res[form]["converged"] and res["c128_rk4"]["converged"]:
+                res[form]["E_rel_vs_c128_converged"] = float(abs(res[form]["E"][0] / res["c128_rk4"]["E"][0] - 1))
+                res[form]["mu_rel_vs_c128_converged"] = float(abs(res[form]["mu"][0] / res["c128_rk4"]["mu"][0] - 1))
+        res["cpu_baseline"] = imag_cpu_leg(name, st)
         out["cases"][name] = res
     print(json.dumps(out))
+
+
+def imag_cpu_leg(name, st, budget_s=8.0):
+    """CPU leg of an imaginary-time case: the FP64 oracle port timed over a
+    bounded number of RK4 imaginary-time iterations from the case's start,
+    and, as the checker, both GPU forms over the same iterations (psi, E, mu
+    relative errors and the norm after renormalisation)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as orc
+    import fgpe_b200 as gp
+    threads = os.cpu_count() or 1
+    orc.set_threads(threads)
+    cfg, V, psis = imag_case(name, gp.C128, gp.IMAG_RK4)
+    o = orc.OracleSolver(cfg)
+    for c in range(cfg.ncomp):
+        o.set_vext(c, V)
+        o.set_psi(c, psis[c])
+    t0 = time.perf_counter()
+    o.step_imag(0, 1)
+    one = time.perf_counter() - t0
+    k = max(1, min(50, int(budget_s / max(one, 1e-3))))
+    t0 = time.perf_counter()
+    o.step_imag(1, k)
+    dt = time.perf_counter() - t0
+    so = o.imag_state()
+    po = [o.get_psi(c) for c in range(cfg.ncomp)]
+    o.close()
+    out = {"value": round(k / dt, 4), "unit": "iterations/s", "cores": threads, "kind": "port",
+           "sample": f"{k + 1} RK4 imaginary-time iterations of the case in FP64 (oracle/gpe_oracle.cpp); {k} timed"}
+    par = {"iterations": k + 1}
+    for form, prec in (("c128_rk4", gp.C128), ("c64_rk4", gp.C64)):
+        cfg2, V2, psis2 = imag_case(name, prec, gp.IMAG_RK4)
+        s = gp.Solver(cfg2)
+        s.set_stream(st.cuda_stream)
+        for c in range(cfg2.ncomp):
+            s.set_vext(c, V2)
+            s.set_psi(c, psis2[c])
+        s.step_imag(0, k + 1)
+        sg = s.imag_state()
+        e = {"psi_rel_l2": [float(np.linalg.norm(s.get_psi(c) - po[c]) / np.linalg.norm(po[c]))
+                            for c in range(cfg2.ncomp)],
+             "E_rel_err": [float(abs(sg[4 * c + 2] / so[4 * c + 2] - 1)) for c in range(cfg2.ncomp)],
+             "mu_rel_err": [float(abs(sg[4 * c + 1] / so[4 * c + 1] - 1)) for c in range(cfg2.ncomp)]}
+        obs = s.observables(0.0)
+        e["norm_rel_err"] = [float(abs(obs[3 * c] / cfg2.npart[c] - 1)) for c in range(cfg2.ncomp)]
+        s.close()
+        par[form] = e
+    out["parity_vs_port"] = par
+    return out
 
 
 def main():

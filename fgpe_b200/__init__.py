@@ -18,7 +18,8 @@ from ctypes import POINTER, byref, c_double, c_int, c_longlong, c_void_p
 import numpy as np
 
 __all__ = [
-    "GPEConfig", "GPEError", "Solver", "lib", "make_config", "grid_axes",
+    "GPEConfig", "GPEError", "Solver", "Batch", "lib", "make_config", "grid_axes", "kspace_kernel", "tune",
+    "set_tune_cache", "pass_variant_exists",
     "C128", "C64", "HAM_BEC", "HAM_BEC2", "HAM_TEMPLATE", "HAM_DIPOLAR",
     "IMAG_HEAVYBALL", "IMAG_RK4", "NO_HAMIL_PARAMS",
 ]
@@ -78,6 +79,7 @@ def lib() -> ctypes.CDLL:
         "gpe_status_string": (ctypes.c_char_p, [c_int]),
         "gpe_config_init": (c_int, [POINTER(GPEConfig)]),
         "gpe_fft_length_supported": (c_int, [c_int]),
+        "gpe_kspace_kernel": (c_int, [POINTER(GPEConfig), P]),
         "gpe_create": (c_int, [POINTER(GPEConfig), POINTER(H)]),
         "gpe_destroy": (c_int, [H]),
         "gpe_set_stream": (c_int, [H, c_void_p]),
@@ -115,6 +117,13 @@ def lib() -> ctypes.CDLL:
         "gpe_batch_step_imag": (c_int, [H, c_int, POINTER(c_int), POINTER(c_int)]),
         "gpe_batch_imag_state": (c_int, [H, c_int, P]),
         "gpe_batch_kernel_launches": (c_longlong, [H]),
+        "gpe_tune": (c_int, [POINTER(GPEConfig), c_int, ctypes.c_char_p, P]),
+        "gpe_set_tune_cache": (c_int, [ctypes.c_char_p]),
+        "gpe_batch_tune": (c_int, [H, ctypes.c_char_p, P]),
+        "gpe_batch_groups": (c_int, [H]),
+        "gpe_get_pass_variants": (c_int, [H, POINTER(c_int)]),
+        "gpe_set_pass_variants": (c_int, [H, POINTER(c_int)]),
+        "gpe_pass_variant_exists": (c_int, [POINTER(GPEConfig), c_int, c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -180,6 +189,36 @@ def make_config(shape, xmax, *, dt=1e-3, ncomp=1, precision=C128, hamiltonian=HA
     c.npart[0], c.npart[1] = npart
     c.epsilon_e = epsilon_e
     return c
+
+
+NSVAR = 12  # strided-pass variants per axis and mode (include/gpe.h, gpe_pass_variant_exists)
+
+
+def tune(cfg: GPEConfig, workload: int = 0, cache_path: str | None = None) -> dict:
+    """Autotune the pass variants of cfg's grid (gpe_tune): workload 0 =
+    real-time RK4 steps, 1 = imaginary-time iterations.  Stores the result
+    in the JSON-lines cache_path when given."""
+    rep = np.zeros(10)
+    _check(lib().gpe_tune(byref(cfg), workload, cache_path.encode() if cache_path else None, _dp(rep)))
+    return {"default_us": float(rep[0]), "tuned_us": float(rep[1]), "timed": int(rep[2]),
+            "variants": [int(x) for x in rep[3:9]], "xrows": int(rep[9])}
+
+
+def set_tune_cache(path: str | None) -> None:
+    """Process-wide cache that new handles and batches apply (None: $GPE_TUNE_CACHE)."""
+    _check(lib().gpe_set_tune_cache(path.encode() if path else None))
+
+
+def pass_variant_exists(cfg: GPEConfig, axis: int, v: int) -> bool:
+    return bool(lib().gpe_pass_variant_exists(byref(cfg), axis, v))
+
+
+def kspace_kernel(cfg: GPEConfig) -> np.ndarray:
+    """V~(k) of a GPE_HAM_DIPOLAR / GPE_HAM_SOFT config as libgpe builds it
+    (host arithmetic, gpe_kspace_kernel), shape (nz, ny, nx)."""
+    out = np.zeros((cfg.nz, cfg.ny, cfg.nx))
+    _check(lib().gpe_kspace_kernel(byref(cfg), _dp(out)))
+    return out
 
 
 class Solver:
@@ -344,6 +383,16 @@ class Solver:
 
     PROF_KINDS = ("x_fwd", "x_inv", "x_full", "s_fwd", "s_inv", "s_fki")
 
+    def pass_variants(self) -> list:
+        """[s(y, fwd), s(y, fki), s(y, inv), s(z, fwd), s(z, fki), s(z, inv), x rows]."""
+        out = (c_int * 7)()
+        _check(lib().gpe_get_pass_variants(self.handle, out))
+        return list(out)
+
+    def set_pass_variants(self, v) -> None:
+        arr = (c_int * 7)(*[int(x) for x in v])
+        _check(lib().gpe_set_pass_variants(self.handle, arr))
+
     def profile(self, enable: bool) -> None:
         _check(lib().gpe_profile_enable(self._h, 1 if enable else 0))
 
@@ -420,6 +469,14 @@ class Batch:
         out = np.zeros(4)
         _check(lib().gpe_batch_imag_state(self._h, i, _dp(out)))
         return out
+
+    def tune(self, cache_path: str | None = None) -> list:
+        """Tune every geometry group in place (gpe_batch_tune): per group
+        (default, tuned) microseconds per imaginary-time iteration."""
+        ng = lib().gpe_batch_groups(self._h)
+        rep = np.zeros(2 * max(ng, 1))
+        _check(lib().gpe_batch_tune(self._h, cache_path.encode() if cache_path else None, _dp(rep)))
+        return [(float(rep[2 * g]), float(rep[2 * g + 1])) for g in range(ng)]
 
     @property
     def launches(self) -> int:

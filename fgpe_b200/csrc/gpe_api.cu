@@ -2,8 +2,10 @@
 // host-side orchestration of the fused pass chains (see include/gpe.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -39,7 +41,8 @@ gpe_status fail(gpe_status s, const std::string& msg) {
 
 bool length_compiled(int L) {
 #define GPE_IS(n) if (L == n) return true;
-    GPE_SIZES_p2(GPE_IS) GPE_SIZES_p3(GPE_IS) GPE_SIZES_p5(GPE_IS) GPE_SIZES_p9(GPE_IS)
+    GPE_SIZES_p2(GPE_IS) GPE_SIZES_p2b(GPE_IS) GPE_SIZES_p3(GPE_IS) GPE_SIZES_p3b(GPE_IS)
+    GPE_SIZES_p5(GPE_IS) GPE_SIZES_p5b(GPE_IS) GPE_SIZES_p9(GPE_IS) GPE_SIZES_p9b(GPE_IS)
 #undef GPE_IS
     return false;
 }
@@ -72,6 +75,12 @@ struct gpe_handle {
     void* W[3] = {nullptr, nullptr, nullptr};
     void* O[4] = {nullptr, nullptr, nullptr, nullptr};
     void* tw[3] = {nullptr, nullptr, nullptr};
+    float4* tw2[3] = {nullptr, nullptr, nullptr};  // complex64: (cos, cos, sin, sin) per axis
+    // pass variants (gpe_tune): svar[axis][mode] for the strided passes
+    // (mode 0 forward, 1 forward*k*inverse, 2 inverse; 0 = default variant),
+    // xrows = rows per CTA of the x passes (0 = default)
+    int svar[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    int xrows = 0;
     double* kax[3] = {nullptr, nullptr, nullptr};
     float* k2s[3] = {nullptr, nullptr, nullptr};  // complex64: lap_scale * k^2 per axis
     double* obs_part = nullptr;                    // OBS_BLOCKS partial sums + the result
@@ -101,6 +110,11 @@ struct gpe_handle {
     double* d_part = nullptr;
     double* d_grad = nullptr;
     std::vector<void*> cps;
+    std::vector<void*> cps_lo;  // complex64: low parts of the checkpoints
+    // imaginary-time chunks: pinned copies of the device's done flag and the
+    // events that mark when each copy has landed
+    int* flag_host = nullptr;
+    cudaEvent_t flag_ev[2] = {nullptr, nullptr};
     // per-pass event timing (gpe_profile_enable)
     bool prof = false;
     std::vector<cudaEvent_t> ev_free;
@@ -279,10 +293,31 @@ __global__ void k_ctrl_final(const double* part, int nblocks, int nv, double* ou
     out[k] = s;
 }
 
+// Spherical real-space cut-off factor of the dipolar kernel,
+// c(q) = 1 + 3cos(q)/q^2 - 3sin(q)/q^3 = 3 int_0^q j2(x)/x dx.  Below q = 0.5
+// the closed form cancels (relative error about 1e-16 * 30/q^4), so there the
+// power series c(q) = 3 sum_n (-1)^n q^(2n+2) / ((2n+2) 2^n n! (2n+5)!!) is
+// summed instead (eight terms: the first omitted one is below 1e-22 of c).
+inline double dipolar_cutoff_factor(double q) {
+    if (q >= 0.5) return 1.0 + 3.0 * std::cos(q) / (q * q) - 3.0 * std::sin(q) / (q * q * q);
+    double sum = 0.0, pw = q * q, fact2n = 1.0, nfact = 1.0, dfact = 15.0;  // 2^n, n!, (2n+5)!!
+    for (int n = 0; n < 8; ++n) {
+        if (n > 0) {
+            fact2n *= 2.0;
+            nfact *= n;
+            dfact *= (2.0 * n + 5.0);
+            pw *= -q * q;
+        }
+        sum += pw / ((2.0 * n + 2.0) * fact2n * nfact * dfact);
+    }
+    return 3.0 * sum;
+}
+
 // Host copy of the dipolar kernel (see gpe_config docs / GPE_HAM_DIPOLAR),
 // the unused DipoleDipoleInteraction of src/parallel.cu:326-352 with a
-// spherical cut-off, divided by N for the unnormalised inverse FFT.
-void host_vdd(const gpe_config& c, const std::vector<double>* k, std::vector<double>& out) {
+// spherical cut-off, divided by N for the unnormalised inverse FFT unless
+// per_n is false (gpe_kspace_kernel returns the kernel itself).
+void host_vdd(const gpe_config& c, const std::vector<double>* k, std::vector<double>& out, bool per_n = true) {
     const long long N = (long long)c.nx * c.ny * c.nz;
     out.assign(N, 0.0);
     if (c.hamiltonian == GPE_HAM_SOFT) {
@@ -304,7 +339,7 @@ void host_vdd(const gpe_config& c, const std::vector<double>* k, std::vector<dou
                         v = kk < 1e-6 ? U * (4. / 3.) * pi * std::pow(a, 3)
                                       : 4 * pi * U * std::pow(a, 3) * (std::sin(kk * a) - kk * a * std::cos(kk * a)) /
                                             std::pow(kk * a, 3);
-                    out[idx] = v / (double)N;
+                    out[idx] = per_n ? v / (double)N : v;
                 }
         return;
     }
@@ -327,10 +362,10 @@ void host_vdd(const gpe_config& c, const std::vector<double>* k, std::vector<dou
                     v = 12.0 * pi * add * ((num / den) * (num / den) - 1.0 / 3.0);
                     if (R > 0) {
                         const double q = 2.0 * pi * den * R;
-                        v *= 1.0 + 3.0 * std::cos(q) / (q * q) - 3.0 * std::sin(q) / (q * q * q);
+                        v *= dipolar_cutoff_factor(q);
                     }
                 }
-                out[idx] = v / (double)N;
+                out[idx] = per_n ? v / (double)N : v;
             }
 }
 
@@ -477,7 +512,8 @@ gpe_status launch_x(gpe_handle* h, PassArgs<R> a, int nf, int mode) {
     a.tw = (const C*)h->tw[0];
     const int L = h->nx;
     const int T = plan_T(L);
-    const int rows = (256 / T) > 0 ? 256 / T : 1;
+    int rows = (256 / T) > 0 ? 256 / T : 1;
+    if (h->xrows > 0 && h->xrows < rows) rows = h->xrows;
     const size_t smem = (size_t)rows * xpad(L) * sizeof(C);
     cudaError_t err = cudaSuccess;
     if (!dispatch_x(L, nf, a, rows, smem, h->st, &err))
@@ -500,6 +536,7 @@ gpe_status launch_s(gpe_handle* h, PassArgs<R> a, int nf, int axis, int mode) {
     a.sax = axis;
     a.tx = tx;
     a.tw = (const C*)h->tw[axis];
+    a.tw2 = h->tw2[axis];
     int nouter;
     if (axis == 1) {
         a.sstride = h->nx;
@@ -510,10 +547,22 @@ gpe_status launch_s(gpe_handle* h, PassArgs<R> a, int nf, int axis, int mode) {
         a.ostride = h->nx;
         nouter = h->ny;
     }
-    const size_t smem = (size_t)L * tx * sizeof(C);
     cudaError_t err = cudaSuccess;
-    if (!dispatch_s(L, nf, a, nouter, smem, h->st, &err))
-        return fail(GPE_ERR_UNSUPPORTED, "no strided-pass kernel for length " + std::to_string(L));
+    bool found = false;
+    // pass variant (gpe_tune): 1 = paired complex64 lines at the default tile
+    // (any length; two-field passes only where both fields' pairs fit the
+    // register budget: 8 values per thread, lines of 64 or more); 2.. = the
+    // tuned lengths' one-field variants; paired variants need an even nx
+    const int mi = mode == SM_FWD ? 0 : (mode == SM_FKI ? 1 : 2);
+    const int v = h->svar[axis][mi];
+    if (v == 1 && sizeof(R) == 4 && h->nx % 2 == 0 && (nf == 1 || (make_plan(L).E <= 8 && L >= 64))) {
+        if constexpr (sizeof(R) == 4)
+            found = dispatch_s2(L, nf, a, nouter, (size_t)L * spass2_txp(L) * sizeof(float4), h->st, &err);
+    } else if (v >= 2 && nf == 1 && (!svar((int)sizeof(C), L, v).paired || h->nx % 2 == 0)) {
+        found = dispatch_sv(L, v, a, nouter, h->st, &err);
+    }
+    if (!found) found = dispatch_s(L, nf, a, nouter, (size_t)L * tx * sizeof(C), h->st, &err);
+    if (!found) return fail(GPE_ERR_UNSUPPORTED, "no strided-pass kernel for length " + std::to_string(L));
     if (err != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("strided pass launch: ") + cudaGetErrorString(err));
     h->launches++;
     return GPE_OK;
@@ -703,10 +752,33 @@ gpe_status imag_issue(gpe_handle* h, int first, int nsteps) {
     return GPE_OK;
 }
 
+// Imaginary-time iterations are issued in chunks of IMAG_CHUNK.  After each
+// chunk an asynchronous copy of the device's done flag (convergence or error)
+// lands in pinned host memory; the host reads the flag of a chunk while the
+// next chunk is already queued, and stops issuing once it is set.  So the
+// device never idles between chunks, and a call that converges early issues
+// at most one chunk past the converging iteration (whose kernels exit at
+// once on the flag) instead of every requested iteration.
+constexpr int IMAG_CHUNK = 64;
+
 template <typename R>
 gpe_status step_imag_t(gpe_handle* h, int first, int nsteps, int* iters_done, int* converged) {
     GPE_TRY(imag_prepare<R>(h));
-    GPE_TRY(imag_issue<R>(h, first, nsteps));
+    int issued = 0, slot = 0, prev = -1;
+    while (issued < nsteps) {
+        const int n = std::min(IMAG_CHUNK, nsteps - issued);
+        GPE_TRY(imag_issue<R>(h, first + issued, n));
+        issued += n;
+        if (issued >= nsteps) break;
+        GPE_CUDA(cudaMemcpyAsync(h->flag_host + slot, &h->sc->done, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+        GPE_CUDA(cudaEventRecord(h->flag_ev[slot], h->st));
+        if (prev >= 0) {
+            GPE_CUDA(cudaEventSynchronize(h->flag_ev[prev]));
+            if (h->flag_host[prev]) break;
+        }
+        prev = slot;
+        slot ^= 1;
+    }
     DevScalars s;
     GPE_TRY(sync_read_scalars(h, &s));
     if (iters_done) *iters_done = s.iters_done;
@@ -844,7 +916,8 @@ gpe_status ensure_out_buffers(gpe_handle* h) {
 
 void free_all(gpe_handle* h) {
     void* ptrs[] = {h->A[0], h->A[1], h->B[0], h->B[1], h->K[0], h->K[1], h->V[0], h->V[1], h->W[0], h->W[1],
-                    h->W[2], h->O[0], h->O[1], h->O[2], h->O[3], h->tw[0], h->tw[1], h->tw[2], h->kax[0],
+                    h->W[2], h->O[0], h->O[1], h->O[2], h->O[3], h->tw[0], h->tw[1], h->tw[2], h->tw2[0],
+                    h->tw2[1], h->tw2[2], h->kax[0],
                     h->kax[1], h->kax[2], h->vdd, h->prms, h->sc, h->partials, h->stage128, h->Lo[0], h->Lo[1],
                     h->k2s[0], h->k2s[1], h->k2s[2], h->obs_part};
     for (void* p : ptrs)
@@ -855,6 +928,11 @@ void free_all(gpe_handle* h) {
         if (p) cudaFree(p);
     for (void* p : h->cps)
         if (p) cudaFree(p);
+    for (void* p : h->cps_lo)
+        if (p) cudaFree(p);
+    if (h->flag_host) cudaFreeHost(h->flag_host);
+    for (cudaEvent_t e : h->flag_ev)
+        if (e) cudaEventDestroy(e);
     for (auto& r : h->recs) {
         cudaEventDestroy(r.a);
         cudaEventDestroy(r.b);
@@ -901,6 +979,19 @@ gpe_status gpe_config_init(gpe_config* cfg) {
 }
 
 int gpe_fft_length_supported(int n) { return (n >= 1 && make_plan(n).ok && length_compiled(n)) ? 1 : 0; }
+
+gpe_status gpe_kspace_kernel(const gpe_config* cfg, double* out) {
+    if (!cfg || !out) return fail(GPE_ERR_INVALID_ARG, "null argument");
+    if (cfg->abi_version != GPE_ABI_VERSION) return fail(GPE_ERR_INVALID_ARG, "abi_version mismatch");
+    if (cfg->hamiltonian != GPE_HAM_DIPOLAR && cfg->hamiltonian != GPE_HAM_SOFT)
+        return fail(GPE_ERR_INVALID_ARG, "the k-space kernel exists for GPE_HAM_DIPOLAR and GPE_HAM_SOFT only");
+    if (cfg->nx < 1 || cfg->ny < 1 || cfg->nz < 1) return fail(GPE_ERR_INVALID_ARG, "grid sizes must be >= 1");
+    std::vector<double> kax[3], v;
+    host_kaxes(*cfg, kax);
+    host_vdd(*cfg, kax, v, false);
+    std::memcpy(out, v.data(), sizeof(double) * v.size());
+    return GPE_OK;
+}
 
 }  // extern "C"
 
@@ -995,6 +1086,10 @@ gpe_status ctrl_reduce_grad(gpe_handle* h, int n) {
     return GPE_OK;
 }
 
+// complex64: the forward steps carry the compensated state (high part in A,
+// low part in Lo, as gpe_step_real does), and the checkpoints keep both
+// parts; the stage arguments of the adjoint are the high parts, as in the
+// forward step.
 template <typename R>
 gpe_status control_gradient_t(gpe_handle* h, const double* host_u, int nsteps, const double* host_target, int K,
                               double* loss_out, double* host_grad) {
@@ -1002,6 +1097,11 @@ gpe_status control_gradient_t(gpe_handle* h, const double* host_u, int nsteps, c
     GPE_TRY(canonicalize_t<R>(h));
     h->w_fwd_A = false;
     h->hb_old_valid = false;
+    const bool comp = sizeof(R) == 4 && h->Lo[0] != nullptr;
+    if (comp && !h->lo_valid) {
+        GPE_CUDA(cudaMemsetAsync(h->Lo[0], 0, h->esz * h->N, h->st));
+        h->lo_valid = true;
+    }
     const size_t fb = h->esz * h->N;
     const int ncp = (nsteps + K - 1) / K + 1;
     // buffers: u, grad, partials, work fields, checkpoints (kept for reuse)
@@ -1020,26 +1120,50 @@ gpe_status control_gradient_t(gpe_handle* h, const double* host_u, int nsteps, c
         GPE_CUDA(cudaMalloc(&p, fb));
         h->cps.push_back(p);
     }
+    while (comp && (int)h->cps_lo.size() < ncp) {
+        void* p = nullptr;
+        GPE_CUDA(cudaMalloc(&p, fb));
+        h->cps_lo.push_back(p);
+    }
     GPE_CUDA(cudaMemcpyAsync(h->d_u, host_u, sizeof(double) * (size_t)nsteps * h->nctrl, cudaMemcpyHostToDevice, h->st));
     GPE_CUDA(cudaMemcpyAsync(h->V0, h->V[0], fb, cudaMemcpyDeviceToDevice, h->st));
     void* target = h->adj[6];
     GPE_TRY(upload_c128_host(h, host_target, target));
     // forward with checkpoints cps[0..ncp-1] (cps[j] = psi at step j*K)
-    GPE_CUDA(cudaMemcpyAsync(h->cps[0], h->A[0], fb, cudaMemcpyDeviceToDevice, h->st));
+    auto save_cp = [&](int j) -> gpe_status {
+        GPE_CUDA(cudaMemcpyAsync(h->cps[j], h->A[0], fb, cudaMemcpyDeviceToDevice, h->st));
+        if (comp) GPE_CUDA(cudaMemcpyAsync(h->cps_lo[j], h->Lo[0], fb, cudaMemcpyDeviceToDevice, h->st));
+        return GPE_OK;
+    };
+    auto load_cp = [&](int j) -> gpe_status {
+        GPE_CUDA(cudaMemcpyAsync(h->A[0], h->cps[j], fb, cudaMemcpyDeviceToDevice, h->st));
+        if (comp) {
+            GPE_CUDA(cudaMemcpyAsync(h->Lo[0], h->cps_lo[j], fb, cudaMemcpyDeviceToDevice, h->st));
+            h->lo_valid = true;
+        }
+        h->w_fwd_A = false;  // A was replaced: W no longer holds its transform
+        return GPE_OK;
+    };
+    GPE_TRY(save_cp(0));
     for (int n = 0; n < nsteps; ++n) {
         GPE_TRY(ctrl_form_v<R>(h, n));
-        GPE_TRY(step_real_t<R>(h, n, 1, nullptr, false));
-        if ((n + 1) % K == 0 && n + 1 < nsteps)
-            GPE_CUDA(cudaMemcpyAsync(h->cps[(n + 1) / K], h->A[0], fb, cudaMemcpyDeviceToDevice, h->st));
+        GPE_TRY(step_real_t<R>(h, n, 1, nullptr, comp));
+        if ((n + 1) % K == 0 && n + 1 < nsteps) GPE_TRY(save_cp((n + 1) / K));
     }
-    // loss = 1 - |o|^2, o = sum conj(target) psi_T DV
-    k_ctrl_partials<C, R><<<CTRL_BLOCKS, 256, 0, h->st>>>(0, (const C*)target, (const C*)h->A[0], nullptr, nullptr, 0,
-                                                         h->N, h->d_part);
-    k_ctrl_final<<<1, 64, 0, h->st>>>(h->d_part, CTRL_BLOCKS, 2, h->d_grad);
-    h->launches += 2;
-    double o[2];
-    GPE_CUDA(cudaMemcpyAsync(o, h->d_grad, sizeof(o), cudaMemcpyDeviceToHost, h->st));
-    GPE_CUDA(cudaStreamSynchronize(h->st));
+    // loss = 1 - |o|^2, o = sum conj(target) psi_T DV (psi_T = high + low part)
+    double o[2] = {0.0, 0.0};
+    for (int part = 0; part < (comp ? 2 : 1); ++part) {
+        k_ctrl_partials<C, R><<<CTRL_BLOCKS, 256, 0, h->st>>>(0, (const C*)target,
+                                                             (const C*)(part ? h->Lo[0] : h->A[0]), nullptr,
+                                                             nullptr, 0, h->N, h->d_part);
+        k_ctrl_final<<<1, 64, 0, h->st>>>(h->d_part, CTRL_BLOCKS, 2, h->d_grad);
+        h->launches += 2;
+        double op[2];
+        GPE_CUDA(cudaMemcpyAsync(op, h->d_grad, sizeof(op), cudaMemcpyDeviceToHost, h->st));
+        GPE_CUDA(cudaStreamSynchronize(h->st));
+        o[0] += op[0];
+        o[1] += op[1];
+    }
     const double DV = h->cfg.dx[0] * h->cfg.dx[1] * h->cfg.dx[2];
     o[0] *= DV;
     o[1] *= DV;
@@ -1052,13 +1176,12 @@ gpe_status control_gradient_t(gpe_handle* h, const double* host_u, int nsteps, c
         void** seg = h->cps.data() + ncp;  // K + 1 states of one segment
         for (int j = (nsteps - 1) / K; j >= 0; --j) {
             const int n0 = j * K, n1 = std::min(nsteps, n0 + K);
-            GPE_CUDA(cudaMemcpyAsync(h->A[0], h->cps[j], fb, cudaMemcpyDeviceToDevice, h->st));
-            h->w_fwd_A = false;  // A was replaced: W no longer holds its transform
+            GPE_TRY(load_cp(j));
             for (int n = n0; n < n1; ++n) {
                 GPE_CUDA(cudaMemcpyAsync(seg[n - n0], h->A[0], fb, cudaMemcpyDeviceToDevice, h->st));
                 if (n + 1 < n1) {
                     GPE_TRY(ctrl_form_v<R>(h, n));
-                    GPE_TRY(step_real_t<R>(h, n, 1, nullptr, false));
+                    GPE_TRY(step_real_t<R>(h, n, 1, nullptr, comp));
                 }
             }
             for (int n = n1 - 1; n >= n0; --n) {
@@ -1072,12 +1195,14 @@ gpe_status control_gradient_t(gpe_handle* h, const double* host_u, int nsteps, c
                                  cudaMemcpyDeviceToHost, h->st));
     }
     // leave psi and V as they were
-    GPE_CUDA(cudaMemcpyAsync(h->A[0], h->cps[0], fb, cudaMemcpyDeviceToDevice, h->st));
+    GPE_TRY(load_cp(0));
     GPE_CUDA(cudaMemcpyAsync(h->V[0], h->V0, fb, cudaMemcpyDeviceToDevice, h->st));
     GPE_CUDA(cudaStreamSynchronize(h->st));
     h->w_fwd_A = false;
     return check_device_status(h);
 }
+
+void tune_apply_cache(gpe_handle* h);  // autotuner section below
 
 // A handle holding nb instances of one configuration (nb > 1: a gpe_batch
 // group; instance i's fields start at element i*N, its parameters, scalars
@@ -1169,6 +1294,10 @@ gpe_status create_handle(const gpe_config* cfg, int nb, gpe_handle** out) {
             host_twiddles(L3[d], tw);
             if (!dmalloc(&h->tw[d], sizeof(float2) * L3[d])) return bail(GPE_ERR_OUT_OF_MEMORY);
             cudaMemcpy(h->tw[d], tw.data(), sizeof(float2) * L3[d], cudaMemcpyHostToDevice);
+            std::vector<float4> tw2(L3[d]);
+            for (int m = 0; m < L3[d]; ++m) tw2[m] = make_float4(tw[m].x, tw[m].x, tw[m].y, tw[m].y);
+            if (!dmalloc((void**)&h->tw2[d], sizeof(float4) * L3[d])) return bail(GPE_ERR_OUT_OF_MEMORY);
+            cudaMemcpy(h->tw2[d], tw2.data(), sizeof(float4) * L3[d], cudaMemcpyHostToDevice);
         }
     }
     if (h->dens) {
@@ -1198,6 +1327,10 @@ gpe_status create_handle(const gpe_config* cfg, int nb, gpe_handle** out) {
         cudaMemcpy(h->sc, sv.data(), sizeof(DevScalars) * nb, cudaMemcpyHostToDevice);
         cudaMemcpy(h->prms, pv.data(), sizeof(double) * pv.size(), cudaMemcpyHostToDevice);
     }
+    if (cudaHostAlloc((void**)&h->flag_host, 2 * sizeof(int), cudaHostAllocDefault) != cudaSuccess)
+        return bail(GPE_ERR_OUT_OF_MEMORY);
+    for (cudaEvent_t& ev : h->flag_ev)
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return bail(GPE_ERR_CUDA);
     const size_t nblk = (size_t)h->ny * h->nz;  // x-pass CTAs hold >= 1 row each
     if (!dmalloc((void**)&h->partials, nblk * MAXQ * 2 * sizeof(double) * nb)) return bail(GPE_ERR_OUT_OF_MEMORY);
     cudaError_t e = cudaDeviceSynchronize();
@@ -1205,6 +1338,7 @@ gpe_status create_handle(const gpe_config* cfg, int nb, gpe_handle** out) {
         g_err = std::string("gpe_create: ") + cudaGetErrorString(e);
         return bail(GPE_ERR_CUDA);
     }
+    tune_apply_cache(h);
     *out = h;
     return GPE_OK;
 }
@@ -1251,7 +1385,7 @@ gpe_status gpe_set_params(gpe_handle* h, const double prms[GPE_NO_HAMIL_PARAMS])
 }
 
 gpe_status gpe_set_psi(gpe_handle* h, int comp, const double* host_c128) {
-    if (h) h->w_fwd_A = h->lo_valid = false;
+    if (h) h->w_fwd_A = false;
     GPE_TRY(check_handle(h));
     GPE_TRY(check_comp(h, comp));
     if (!host_c128) return fail(GPE_ERR_INVALID_ARG, "null psi");
@@ -1265,7 +1399,7 @@ gpe_status gpe_set_psi(gpe_handle* h, int comp, const double* host_c128) {
 }
 
 gpe_status gpe_set_psi_device(gpe_handle* h, int comp, const void* dev_c128) {
-    if (h) h->w_fwd_A = h->lo_valid = false;
+    if (h) h->w_fwd_A = false;
     GPE_TRY(check_handle(h));
     GPE_TRY(check_comp(h, comp));
     if (!dev_c128) return fail(GPE_ERR_INVALID_ARG, "null psi");
@@ -1793,5 +1927,401 @@ long long gpe_batch_kernel_launches(const gpe_batch* b) {
     for (const gpe_handle* h : b->groups) n += h->launches;
     return n;
 }
+
+}  // extern "C"
+
+// ==========================================================================================
+// Autotuner: pass variants per grid (no counterpart in the reference, which
+// leaves the transform plan to cuFFT's planner, src/parallel.cu:77-110).
+//
+// For a grid, precision and field count the tuner times, on a temporary
+// handle, every strided-pass variant (svar: scalar or paired complex64 lines,
+// tile width, resident CTAs per SM, radix order) of each strided axis and pass
+// mode with CUDA events, keeps the fastest, then times whole steps of the
+// workload (real-time RK4 steps or imaginary-time iterations) for each
+// x-pass row count per CTA (which sets how full the x pass's last wave is),
+// and keeps the fastest.  The result is one line of a JSON-lines cache,
+// keyed by (nx, ny, nz, precision, fields, instances), which gpe_create and
+// gpe_batch_create apply when a cache is set (gpe_set_tune_cache or
+// $GPE_TUNE_CACHE).  Without a cache every handle uses the default variants.
+// ==========================================================================================
+#include <fstream>
+#include <mutex>
+#include <sstream>
+
+namespace {
+
+std::mutex g_tune_mu;
+std::string g_tune_path;
+bool g_tune_path_set = false;
+
+std::string tune_cache_path() {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    if (g_tune_path_set) return g_tune_path;
+    const char* env = std::getenv("GPE_TUNE_CACHE");
+    return env ? std::string(env) : std::string();
+}
+
+bool length_tuned(int L) {
+#define GPE_IS(n) if (L == n) return true;
+    GPE_TUNED_p2(GPE_IS) GPE_TUNED_p2b(GPE_IS) GPE_TUNED_p3(GPE_IS) GPE_TUNED_p3b(GPE_IS)
+    GPE_TUNED_p5(GPE_IS) GPE_TUNED_p5b(GPE_IS) GPE_TUNED_p9(GPE_IS) GPE_TUNED_p9b(GPE_IS)
+#undef GPE_IS
+    return false;
+}
+
+// Whether strided-pass variant v can serve axis `axis` of handle h (see launch_s).
+bool variant_usable(const gpe_handle* h, int axis, int v) {
+    const int L = axis == 1 ? h->ny : h->nz;
+    const int esz = (int)h->esz;
+    if (v == 0) return true;
+    if (v == 1)
+        return esz == 8 && h->nx % 2 == 0 && (h->nf == 1 || (make_plan(L).E <= 8 && L >= 64));
+    if (v < 0 || v >= NSVAR || h->nf != 1 || !length_tuned(L)) return false;
+    const SVar s = svar(esz, L, v);
+    return s.ok && (!s.paired || h->nx % 2 == 0);
+}
+
+struct TuneKey {
+    int nx, ny, nz, prec, nf, nb;
+};
+TuneKey tune_key(const gpe_handle* h) { return TuneKey{h->nx, h->ny, h->nz, h->prec, h->nf, h->nb}; }
+
+bool json_int(const std::string& line, const char* key, int* out) {
+    const std::string k = std::string("\"") + key + "\":";
+    const size_t p = line.find(k);
+    if (p == std::string::npos) return false;
+    char* end = nullptr;
+    const long v = std::strtol(line.c_str() + p + k.size(), &end, 10);
+    if (end == line.c_str() + p + k.size()) return false;
+    *out = (int)v;
+    return true;
+}
+
+bool line_key(const std::string& line, TuneKey* k) {
+    return json_int(line, "nx", &k->nx) && json_int(line, "ny", &k->ny) && json_int(line, "nz", &k->nz) &&
+           json_int(line, "prec", &k->prec) && json_int(line, "nf", &k->nf) && json_int(line, "nb", &k->nb);
+}
+bool same_key(const TuneKey& a, const TuneKey& b) {
+    return a.nx == b.nx && a.ny == b.ny && a.nz == b.nz && a.prec == b.prec && a.nf == b.nf && a.nb == b.nb;
+}
+
+std::string tune_line(const gpe_handle* h, double def_us, double tuned_us) {
+    std::ostringstream o;
+    const TuneKey k = tune_key(h);
+    o << "{\"nx\":" << k.nx << ",\"ny\":" << k.ny << ",\"nz\":" << k.nz << ",\"prec\":" << k.prec
+      << ",\"nf\":" << k.nf << ",\"nb\":" << k.nb;
+    for (int ax = 1; ax <= 2; ++ax)
+        for (int m = 0; m < 3; ++m) o << ",\"s" << ax << m << "\":" << h->svar[ax][m];
+    o << ",\"xrows\":" << h->xrows;
+    char buf[64];
+    std::snprintf(buf, sizeof(buf), ",\"default_us\":%.3f,\"tuned_us\":%.3f}", def_us, tuned_us);
+    o << buf;
+    return o.str();
+}
+
+// Applies the cache line of h's key, if any (the last one in the file wins).
+// Variants that do not exist for h are ignored.
+void tune_apply_cache(gpe_handle* h) {
+    const std::string path = tune_cache_path();
+    if (path.empty()) return;
+    std::ifstream f(path);
+    if (!f) return;
+    const TuneKey want = tune_key(h);
+    std::string line, hit;
+    while (std::getline(f, line)) {
+        TuneKey k;
+        if (line_key(line, &k) && same_key(k, want)) hit = line;
+    }
+    if (hit.empty()) return;
+    for (int ax = 1; ax <= 2; ++ax)
+        for (int m = 0; m < 3; ++m) {
+            const std::string key = "s" + std::to_string(ax) + std::to_string(m);
+            int v = 0;
+            if (json_int(hit, key.c_str(), &v) && variant_usable(h, ax, v)) h->svar[ax][m] = v;
+        }
+    int r = 0;
+    if (json_int(hit, "xrows", &r) && r >= 0 && r <= 256) h->xrows = r;
+}
+
+// Replaces the line of h's key in the cache file (or appends it).
+gpe_status tune_store(const gpe_handle* h, const char* path, double def_us, double tuned_us) {
+    if (!path || !path[0]) return GPE_OK;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    std::vector<std::string> keep;
+    {
+        std::ifstream f(path);
+        std::string line;
+        const TuneKey want = tune_key(h);
+        while (f && std::getline(f, line)) {
+            TuneKey k;
+            if (line.empty() || (line_key(line, &k) && same_key(k, want))) continue;
+            keep.push_back(line);
+        }
+    }
+    keep.push_back(tune_line(h, def_us, tuned_us));
+    const std::string tmp = std::string(path) + ".tmp";
+    {
+        std::ofstream o(tmp, std::ios::trunc);
+        if (!o) return fail(GPE_ERR_IO, std::string("cannot write ") + tmp);
+        for (const auto& l : keep) o << l << "\n";
+        if (!o) return fail(GPE_ERR_IO, std::string("cannot write ") + tmp);
+    }
+    if (std::rename(tmp.c_str(), path) != 0) return fail(GPE_ERR_IO, std::string("cannot replace ") + path);
+    return GPE_OK;
+}
+
+// A normalised uniform state in every instance and component: the tuning
+// handle's steps then run their full arithmetic (no zero norms).
+template <typename C>
+__global__ void k_fill_const(C* dst, double v, long long n) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = from_d<C>(make_double2(v, 0.0));
+}
+
+// Microseconds per launch of one strided pass (3 untimed launches, then 20).
+template <typename R>
+gpe_status time_pass(gpe_handle* h, int axis, int mode, double* us) {
+    PassArgs<R> a = base_args<R>(h);
+    a.pro = PRO_PIN;
+    a.epi = EPI_STORE;
+    for (int i = 0; i < 3; ++i) GPE_TRY(launch_s<R>(h, a, h->nf, axis, mode));
+    cudaEvent_t e0, e1;
+    GPE_CUDA(cudaEventCreate(&e0));
+    GPE_CUDA(cudaEventCreate(&e1));
+    cudaEventRecord(e0, h->st);
+    gpe_status s = GPE_OK;
+    for (int i = 0; i < 20 && s == GPE_OK; ++i) s = launch_s<R>(h, a, h->nf, axis, mode);
+    cudaEventRecord(e1, h->st);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (s != GPE_OK) return s;
+    if (e != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("tuner timing: ") + cudaGetErrorString(e));
+    *us = 1e3 * ms / 20.0;
+    return GPE_OK;
+}
+
+// Microseconds per step of the workload: 0 real-time RK4 steps, 1 imaginary-
+// time iterations of the handle's scheme (the tuning config never converges).
+// Median of three groups of 10 steps after 3 untimed ones.
+template <typename R>
+gpe_status time_steps(gpe_handle* h, int workload, double* us) {
+    auto issue = [&](int n) -> gpe_status {
+        if (workload == 0) return step_real_t<R>(h, 0, n, nullptr);
+        GPE_TRY(imag_prepare<R>(h));
+        return imag_issue<R>(h, 0, n);
+    };
+    GPE_TRY(issue(3));
+    double t[3];
+    for (int r = 0; r < 3; ++r) {
+        cudaEvent_t e0, e1;
+        GPE_CUDA(cudaEventCreate(&e0));
+        GPE_CUDA(cudaEventCreate(&e1));
+        cudaEventRecord(e0, h->st);
+        gpe_status s = issue(10);
+        cudaEventRecord(e1, h->st);
+        cudaError_t e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (s != GPE_OK) return s;
+        if (e != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("tuner timing: ") + cudaGetErrorString(e));
+        t[r] = 1e3 * ms / 10.0;
+    }
+    std::sort(t, t + 3);
+    *us = t[1];
+    return GPE_OK;
+}
+
+// Tunes handle h (a temporary of the config to tune) in place.
+template <typename R>
+gpe_status tune_handle_t(gpe_handle* h, int workload, double* report) {
+    typedef typename Cx<R>::T C;
+    const double DV = h->cfg.dx[0] * h->cfg.dx[1] * h->cfg.dx[2];
+    const double amp = std::sqrt(h->cfg.npart[0] / ((double)h->N * DV));
+    for (int c = 0; c < h->ncomp; ++c) {
+        k_fill_const<C><<<blocks_for(h->N * h->nb, 256), 256, 0, h->st>>>((C*)h->A[c], amp, h->N * h->nb);
+        k_fill_const<C><<<blocks_for(h->N * h->nb, 256), 256, 0, h->st>>>((C*)h->B[c], amp, h->N * h->nb);
+    }
+    GPE_CUDA(cudaGetLastError());
+    GPE_CUDA(cudaStreamSynchronize(h->st));
+    h->hb_old_valid = true;
+    double def_us = 0.0;
+    GPE_TRY(time_steps<R>(h, workload, &def_us));
+    int timed = 0;
+    int axes[2], na = 0;
+    if (h->ny > 1) axes[na++] = 1;
+    if (h->nz > 1) axes[na++] = 2;
+    for (int i = 0; i < na; ++i) {
+        const int ax = axes[i];
+        const int modes[2] = {SM_FWD, SM_INV};
+        const int nm = (i == na - 1) ? 1 : 2;
+        for (int j = 0; j < nm; ++j) {
+            const int mode = (i == na - 1) ? SM_FKI : modes[j];
+            const int mi = mode == SM_FWD ? 0 : (mode == SM_FKI ? 1 : 2);
+            int best = 0;
+            double best_us = 1e30;
+            for (int v = 0; v < NSVAR; ++v) {
+                if (!variant_usable(h, ax, v)) continue;
+                h->svar[ax][mi] = v;
+                double us = 0.0;
+                if (time_pass<R>(h, ax, mode, &us) != GPE_OK) {
+                    cudaGetLastError();
+                    continue;
+                }
+                ++timed;
+                if (us < best_us * 0.99) {
+                    best_us = us;
+                    best = v;
+                }
+            }
+            h->svar[ax][mi] = best;
+        }
+    }
+    // x-pass rows per CTA: whole steps with the chosen strided variants
+    const int T = plan_T(h->nx);
+    const int rmax = (256 / T) > 0 ? 256 / T : 1;
+    int best_r = 0;
+    double best_us = 1e30;
+    for (int r = rmax; r >= 1 && r >= rmax / 2; --r) {
+        h->xrows = (r == rmax) ? 0 : r;
+        double us = 0.0;
+        GPE_TRY(time_steps<R>(h, workload, &us));
+        ++timed;
+        if (us < best_us * 0.99) {
+            best_us = us;
+            best_r = h->xrows;
+        }
+    }
+    h->xrows = best_r;
+    double tuned_us = 0.0;
+    GPE_TRY(time_steps<R>(h, workload, &tuned_us));
+    if (report) {
+        report[0] = def_us;
+        report[1] = tuned_us;
+        report[2] = timed;
+    }
+    return GPE_OK;
+}
+
+// Tunes a temporary handle of cfg with nb instances; variants out in *h_out
+// (the caller destroys it).
+gpe_status tune_config(const gpe_config* cfg, int nb, int workload, double* report, gpe_handle** h_out) {
+    gpe_config c = *cfg;
+    c.epsilon_e = -1.0;  // never converges: every timed iteration does its work
+    gpe_handle* h = nullptr;
+    GPE_TRY(create_handle(&c, nb, &h));
+    for (int ax = 0; ax < 3; ++ax)
+        for (int m = 0; m < 3; ++m) h->svar[ax][m] = 0;
+    h->xrows = 0;
+    gpe_status s = h->prec == GPE_C64 ? tune_handle_t<float>(h, workload, report)
+                                      : tune_handle_t<double>(h, workload, report);
+    if (s != GPE_OK) {
+        cudaStreamSynchronize(h->st);
+        free_all(h);
+        delete h;
+        return s;
+    }
+    *h_out = h;
+    return GPE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gpe_status gpe_set_tune_cache(const char* path) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_path_set = path != nullptr;
+    g_tune_path = path ? path : "";
+    return GPE_OK;
+}
+
+gpe_status gpe_tune(const gpe_config* cfg, int workload, const char* cache_path, double* report) {
+    if (!cfg) return fail(GPE_ERR_INVALID_ARG, "null config");
+    if (workload != 0 && workload != 1) return fail(GPE_ERR_INVALID_ARG, "workload must be 0 (real) or 1 (imaginary)");
+    gpe_handle* h = nullptr;
+    double rep[3] = {0, 0, 0};
+    GPE_TRY(tune_config(cfg, 1, workload, rep, &h));
+    gpe_status s = tune_store(h, cache_path, rep[0], rep[1]);
+    if (report) {
+        report[0] = rep[0];
+        report[1] = rep[1];
+        report[2] = rep[2];
+        for (int ax = 1; ax <= 2; ++ax)
+            for (int m = 0; m < 3; ++m) report[3 + (ax - 1) * 3 + m] = h->svar[ax][m];
+        report[9] = h->xrows;
+    }
+    cudaStreamSynchronize(h->st);
+    free_all(h);
+    delete h;
+    return s;
+}
+
+gpe_status gpe_get_pass_variants(const gpe_handle* h, int* out) {
+    if (!h || !out) return fail(GPE_ERR_INVALID_ARG, "null argument");
+    for (int ax = 1; ax <= 2; ++ax)
+        for (int m = 0; m < 3; ++m) out[(ax - 1) * 3 + m] = h->svar[ax][m];
+    out[6] = h->xrows;
+    return GPE_OK;
+}
+
+gpe_status gpe_set_pass_variants(gpe_handle* h, const int* in) {
+    if (!h || !in) return fail(GPE_ERR_INVALID_ARG, "null argument");
+    for (int ax = 1; ax <= 2; ++ax)
+        for (int m = 0; m < 3; ++m)
+            if (!variant_usable(h, ax, in[(ax - 1) * 3 + m]))
+                return fail(GPE_ERR_UNSUPPORTED, "pass variant " + std::to_string(in[(ax - 1) * 3 + m]) +
+                                                     " does not exist for axis " + std::to_string(ax));
+    if (in[6] < 0 || in[6] > 256) return fail(GPE_ERR_INVALID_ARG, "xrows must be 0..256");
+    for (int ax = 1; ax <= 2; ++ax)
+        for (int m = 0; m < 3; ++m) h->svar[ax][m] = in[(ax - 1) * 3 + m];
+    h->xrows = in[6];
+    return GPE_OK;
+}
+
+int gpe_pass_variant_exists(const gpe_config* cfg, int axis, int v) {
+    if (!cfg || axis < 1 || axis > 2) return 0;
+    gpe_handle tmp;
+    tmp.nx = cfg->nx;
+    tmp.ny = cfg->ny;
+    tmp.nz = cfg->nz;
+    tmp.esz = cfg->precision == GPE_C64 ? 8 : 16;
+    tmp.nf = cfg->ncomp + ((cfg->hamiltonian == GPE_HAM_DIPOLAR || cfg->hamiltonian == GPE_HAM_SOFT) ? 1 : 0);
+    const int L = axis == 1 ? cfg->ny : cfg->nz;
+    if (L <= 1) return v == 0 ? 1 : 0;
+    return variant_usable(&tmp, axis, v) ? 1 : 0;
+}
+
+gpe_status gpe_batch_tune(gpe_batch* b, const char* cache_path, double* report) {
+    if (!b) return fail(GPE_ERR_INVALID_ARG, "null batch");
+    for (size_t g = 0; g < b->groups.size(); ++g) {
+        gpe_handle* hg = b->groups[g];
+        gpe_handle* t = nullptr;
+        double rep[3] = {0, 0, 0};
+        GPE_TRY(tune_config(&hg->cfg, hg->nb, 1, rep, &t));
+        for (int ax = 0; ax < 3; ++ax)
+            for (int m = 0; m < 3; ++m) hg->svar[ax][m] = t->svar[ax][m];
+        hg->xrows = t->xrows;
+        gpe_status s = tune_store(t, cache_path, rep[0], rep[1]);
+        cudaStreamSynchronize(t->st);
+        free_all(t);
+        delete t;
+        GPE_TRY(s);
+        if (report) {
+            report[2 * g] = rep[0];
+            report[2 * g + 1] = rep[1];
+        }
+    }
+    batch_drop_graph(b);  // the captured iteration holds the old kernels
+    b->use_graph = true;
+    return GPE_OK;
+}
+
+int gpe_batch_groups(const gpe_batch* b) { return b ? (int)b->groups.size() : 0; }
 
 }  // extern "C"

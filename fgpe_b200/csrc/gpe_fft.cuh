@@ -30,25 +30,59 @@ __host__ __device__ constexpr int lcm_c(int a, int b) { return a / gcd_c(a, b) *
 
 // Plan: powers of two use radix 8 with one trailing 4 or 2 (E = 8); lengths
 // with factors 3 or 5 use radix 4 (and one 2) for the power-of-two part so that
-// E = lcm(radices) stays <= 24.
-__host__ __device__ constexpr PlanSpec make_plan(int L) {
+// E = lcm(radices) stays <= 24.  pv selects an alternative radix order for the
+// autotuner (same radices or smaller ones, other placement):
+//   powers of two: 1 = the 4 or 2 first, then the 8s; 2 = radix 4s (and one
+//                  trailing 2: E = 4);
+//   mixed:         1 = the 3s and 5s first; 2 = the 2 first, then 4s, 3s, 5s.
+// A variant that gives no plan (or the default's order) has ok = 0.
+__host__ __device__ constexpr PlanSpec make_plan(int L, int pv = 0) {
     PlanSpec p{0, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}, 1, 0};
-    if (L < 1) return p;
-    if (L == 1) { p.ok = 1; p.E = 1; return p; }
+    if (L < 1 || pv < 0 || pv > 2) return p;
+    if (L == 1) {
+        p.ok = pv == 0 ? 1 : 0;
+        p.E = 1;
+        return p;
+    }
     int m = L, p2 = 0, n3 = 0, n5 = 0;
     while (m % 2 == 0) { m /= 2; ++p2; }
     while (m % 3 == 0) { m /= 3; ++n3; }
     while (m % 5 == 0) { m /= 5; ++n5; }
     if (m != 1) return p;
     if (n3 == 0 && n5 == 0) {
-        while (p2 >= 3) { p.R[p.M++] = 8; p2 -= 3; }
-        if (p2 == 2) p.R[p.M++] = 4;
-        if (p2 == 1) p.R[p.M++] = 2;
+        if (pv == 2) {
+            if (p2 < 3) return p;
+            while (p2 >= 2) { p.R[p.M++] = 4; p2 -= 2; }
+            if (p2 == 1) p.R[p.M++] = 2;
+        } else {
+            const int lead = p2 % 3;  // the 4 or 2
+            if (pv == 1) {
+                if (lead == 0 || p2 < 3) return p;
+                p.R[p.M++] = lead == 2 ? 4 : 2;
+            }
+            while (p2 >= 3) { p.R[p.M++] = 8; p2 -= 3; }
+            if (pv == 0) {
+                if (p2 == 2) p.R[p.M++] = 4;
+                if (p2 == 1) p.R[p.M++] = 2;
+            }
+        }
     } else {
+        const bool two = p2 % 2 == 1;
+        if (pv == 1) {
+            if (p2 == 0) return p;
+            for (int i = 0; i < n3; ++i) p.R[p.M++] = 3;
+            for (int i = 0; i < n5; ++i) p.R[p.M++] = 5;
+        }
+        if (pv == 2) {
+            if (!two || p2 < 3) return p;
+            p.R[p.M++] = 2;
+        }
         while (p2 >= 2) { p.R[p.M++] = 4; p2 -= 2; }
-        if (p2 == 1) p.R[p.M++] = 2;
-        for (int i = 0; i < n3; ++i) p.R[p.M++] = 3;
-        for (int i = 0; i < n5; ++i) p.R[p.M++] = 5;
+        if (pv != 2 && p2 == 1) p.R[p.M++] = 2;
+        if (pv != 1) {
+            for (int i = 0; i < n3; ++i) p.R[p.M++] = 3;
+            for (int i = 0; i < n5; ++i) p.R[p.M++] = 5;
+        }
     }
     if (p.M > 12) return p;
     int e = 1;
@@ -59,9 +93,9 @@ __host__ __device__ constexpr PlanSpec make_plan(int L) {
     return p;
 }
 
-template <int L>
+template <int L, int PV = 0>
 struct Plan {
-    static constexpr PlanSpec spec = make_plan(L);
+    static constexpr PlanSpec spec = make_plan(L, PV);
     static_assert(spec.ok, "FFT length has no plan");
     static constexpr int M = spec.M;
     static constexpr int E = spec.E;
@@ -86,6 +120,12 @@ template <int L, int E, int T, int Rr>
 __device__ __forceinline__ int reg_pos(int t, int e) {
     return t + reg_off<L, E, T, Rr>(e);
 }
+
+// Real component type of a complex type C (float / double; the paired
+// complex64 type of gpe_pair.cuh specialises it to float), and the type its
+// twiddle table holds (C itself here; a broadcast pair for the paired type).
+template <typename C> struct RealOf { typedef decltype(C().x) T; };
+template <typename C> struct TwOf { typedef C T; };
 
 // ---- small DFTs, X_q = sum_r x_r exp(SIGN 2 pi i r q / R) ------------------
 // i*SIGN*b
@@ -116,7 +156,7 @@ template <int SIGN, typename C> struct Butterfly<4, SIGN, C> {
 
 template <int SIGN, typename C> struct Butterfly<8, SIGN, C> {
     __device__ __forceinline__ static void run(C* v) {
-        typedef decltype(v[0].x) R;
+        typedef typename RealOf<C>::T R;
         const R h = (R)0.70710678118654752440084436210484903928;  // 1/sqrt(2)
         C e[4] = {v[0], v[2], v[4], v[6]};
         C o[4] = {v[1], v[3], v[5], v[7]};
@@ -141,7 +181,7 @@ template <int SIGN, typename C> struct Butterfly<8, SIGN, C> {
 
 template <int SIGN, typename C> struct Butterfly<3, SIGN, C> {
     __device__ __forceinline__ static void run(C* v) {
-        typedef decltype(v[0].x) R;
+        typedef typename RealOf<C>::T R;
         const R s3 = (R)0.86602540378443864676372317075293618;  // sin(2 pi/3)
         C t1 = cadd(v[1], v[2]);
         C t2 = mk(v[0].x - (R)0.5 * t1.x, v[0].y - (R)0.5 * t1.y);
@@ -155,7 +195,7 @@ template <int SIGN, typename C> struct Butterfly<3, SIGN, C> {
 
 template <int SIGN, typename C> struct Butterfly<5, SIGN, C> {
     __device__ __forceinline__ static void run(C* v) {
-        typedef decltype(v[0].x) R;
+        typedef typename RealOf<C>::T R;
         const R c1 = (R)0.30901699437494742410229341718281906;   // cos(2 pi/5)
         const R c2 = (R)-0.80901699437494742410229341718281906;  // cos(4 pi/5)
         const R s1 = (R)0.95105651629515357211643933337938214;   // sin(2 pi/5)
@@ -179,15 +219,16 @@ template <int SIGN, typename C> struct Butterfly<5, SIGN, C> {
 // tw: forward roots of unity exp(-2 pi i m/L), m in [0, L).
 // Index arithmetic is unsigned so that (t + q*T) / Ns and % Ns split into a
 // per-thread part and a compile-time part whenever T is a multiple of Ns.
-template <int L, int P, int SIGN, bool REV, typename C, typename Addr>
-__device__ __forceinline__ void fft_passes(C (&v)[Plan<L>::E], const Addr& addr, const C* __restrict__ tw,
-                                           unsigned t) {
-    constexpr int M = Plan<L>::M;
+template <int L, int P, int SIGN, bool REV, int PV, typename C, typename Addr>
+__device__ __forceinline__ void fft_passes(C (&v)[Plan<L, PV>::E], const Addr& addr,
+                                           const typename TwOf<C>::T* __restrict__ tw, unsigned t) {
+    typedef Plan<L, PV> PL;
+    constexpr int M = PL::M;
     if constexpr (P < M) {
-        constexpr int R = Plan<L>::radix(P, REV);
-        constexpr int Ns = Plan<L>::ns(P, REV);
-        constexpr int E = Plan<L>::E;
-        constexpr int T = Plan<L>::T;
+        constexpr int R = PL::radix(P, REV);
+        constexpr int Ns = PL::ns(P, REV);
+        constexpr int E = PL::E;
+        constexpr int T = PL::T;
         constexpr int G = E / R;
         if constexpr (P > 0) {
 #pragma unroll
@@ -202,7 +243,7 @@ __device__ __forceinline__ void fft_passes(C (&v)[Plan<L>::E], const Addr& addr,
                 const unsigned k = j % (unsigned)Ns;
 #pragma unroll
                 for (int r = 1; r < R; ++r) {
-                    const C w = __ldg(tw + (unsigned)r * k * (unsigned)(L / (Ns * R)));
+                    const typename TwOf<C>::T w = __ldg(tw + (unsigned)r * k * (unsigned)(L / (Ns * R)));
                     v[q * R + r] = (SIGN < 0) ? cmul(v[q * R + r], w) : cmulc(v[q * R + r], w);
                 }
             }
@@ -219,23 +260,23 @@ __device__ __forceinline__ void fft_passes(C (&v)[Plan<L>::E], const Addr& addr,
                 for (int r = 0; r < R; ++r) *addr(idxD + (unsigned)(r * Ns)) = v[q * R + r];
             }
             __syncthreads();
-            fft_passes<L, P + 1, SIGN, REV>(v, addr, tw, t);
+            fft_passes<L, P + 1, SIGN, REV, PV>(v, addr, tw, t);
         }
     }
 }
 
 // Forward transform: registers in in_radix(false) pattern -> out_radix(false) pattern.
-template <int L, typename C, typename Addr>
-__device__ __forceinline__ void line_fft_fwd(C (&v)[Plan<L>::E], const Addr& addr, const C* __restrict__ tw,
-                                             unsigned t) {
-    fft_passes<L, 0, -1, false>(v, addr, tw, t);
+template <int L, int PV = 0, typename C, typename Addr>
+__device__ __forceinline__ void line_fft_fwd(C (&v)[Plan<L, PV>::E], const Addr& addr,
+                                             const typename TwOf<C>::T* __restrict__ tw, unsigned t) {
+    fft_passes<L, 0, -1, false, PV>(v, addr, tw, t);
 }
 // Inverse (unnormalised) transform with the radices reversed:
 // registers in in_radix(true) == out_radix(false) pattern -> out_radix(true) == in_radix(false).
-template <int L, typename C, typename Addr>
-__device__ __forceinline__ void line_fft_inv(C (&v)[Plan<L>::E], const Addr& addr, const C* __restrict__ tw,
-                                             unsigned t) {
-    fft_passes<L, 0, +1, true>(v, addr, tw, t);
+template <int L, int PV = 0, typename C, typename Addr>
+__device__ __forceinline__ void line_fft_inv(C (&v)[Plan<L, PV>::E], const Addr& addr,
+                                             const typename TwOf<C>::T* __restrict__ tw, unsigned t) {
+    fft_passes<L, 0, +1, true, PV>(v, addr, tw, t);
 }
 
 }  // namespace gpe

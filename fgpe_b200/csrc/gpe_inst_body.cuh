@@ -1,6 +1,8 @@
 // gpe_inst_body.cuh -- included by gpe_inst_*.cu after defining GPE_R (float
 // or double), GPE_SFX (f or d), GPE_FAM (length family), GPE_NF (fields per
-// pass, 1 or 2) and GPE_SIZES(X).
+// pass, 1 or 2), GPE_SIZES(X) and GPE_TUNED(X) (the family's lengths with
+// autotuner variants); GPE_PAIRED (complex64 units) adds the paired strided
+// passes.
 #include "gpe_kernels_impl.cuh"
 
 #define GPE_CAT2(a, b) a##b
@@ -33,5 +35,37 @@ bool GPE_NAME(dispatch_s_)(int L, const PassArgs<GPE_R>& a, int nouter, size_t s
             return false;
     }
 }
+
+#if GPE_NF == 1
+#define GPE_SVCASE(L)                                                   \
+    case L:                                                             \
+        *err = launch_svar<GPE_R, L>(v, a, nouter, st, &found);         \
+        return found;
+// Autotuner variants of the one-field strided pass at the tuned lengths.
+bool GPE_NAME(dispatch_sv_)(int L, int v, const PassArgs<GPE_R>& a, int nouter, cudaStream_t st, cudaError_t* err) {
+    bool found = false;
+    switch (L) {
+        GPE_TUNED(GPE_SVCASE)
+        default:
+            return false;
+    }
+}
+#endif
+
+#ifdef GPE_PAIRED
+#define GPE_S2CASE(L)                                            \
+    case L:                                                      \
+        *err = launch_spass2<L, GPE_NF>(a, nouter, smem, st);    \
+        return true;
+// Paired complex64 strided passes (two lines per thread, nx even).
+bool GPE_NAME(dispatch_s2_)(int L, const PassArgs<float>& a, int nouter, size_t smem, cudaStream_t st,
+                            cudaError_t* err) {
+    switch (L) {
+        GPE_SIZES(GPE_S2CASE)
+        default:
+            return false;
+    }
+}
+#endif
 
 }  // namespace gpe

@@ -5,4 +5,5 @@
 #define GPE_FAM p2
 #define GPE_NF 1
 #define GPE_SIZES(X) GPE_SIZES_p2(X)
+#define GPE_TUNED(X) GPE_TUNED_p2(X)
 #include "gpe_inst_body.cuh"

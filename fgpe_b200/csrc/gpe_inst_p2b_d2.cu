@@ -1,0 +1,9 @@
+// Pass-kernel instantiations: length family p2b, double, 2 field(s) per pass.
+#include "gpe_sizes.h"
+#define GPE_R double
+#define GPE_SFX d
+#define GPE_FAM p2b
+#define GPE_NF 2
+#define GPE_SIZES(X) GPE_SIZES_p2b(X)
+#define GPE_TUNED(X) GPE_TUNED_p2b(X)
+#include "gpe_inst_body.cuh"

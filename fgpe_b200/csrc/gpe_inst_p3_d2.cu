@@ -5,4 +5,5 @@
 #define GPE_FAM p3
 #define GPE_NF 2
 #define GPE_SIZES(X) GPE_SIZES_p3(X)
+#define GPE_TUNED(X) GPE_TUNED_p3(X)
 #include "gpe_inst_body.cuh"

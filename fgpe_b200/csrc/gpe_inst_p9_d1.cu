@@ -5,4 +5,5 @@
 #define GPE_FAM p9
 #define GPE_NF 1
 #define GPE_SIZES(X) GPE_SIZES_p9(X)
+#define GPE_TUNED(X) GPE_TUNED_p9(X)
 #include "gpe_inst_body.cuh"

@@ -1,8 +1,10 @@
 // Pass-kernel instantiations: length family p9, float, 2 field(s) per pass.
 #include "gpe_sizes.h"
 #define GPE_R float
+#define GPE_PAIRED 1
 #define GPE_SFX f
 #define GPE_FAM p9
 #define GPE_NF 2
 #define GPE_SIZES(X) GPE_SIZES_p9(X)
+#define GPE_TUNED(X) GPE_TUNED_p9(X)
 #include "gpe_inst_body.cuh"

@@ -20,6 +20,7 @@
 
 #include "gpe_common.cuh"
 #include "gpe_fft.cuh"
+#include "gpe_pair.cuh"
 #include "../../include/gpe.h"
 
 namespace gpe {
@@ -80,6 +81,7 @@ struct PassArgs {
     const C* vext[2];
     C* out[4];               // EPI_APPLYH: h_mu c0, h_en c0, h_mu c1, h_en c1
     const C* tw;             // roots of unity for this pass's length
+    const float4* tw2;       // complex64: the same roots as (cos, cos, sin, sin) for the paired passes
     const double* kx;
     const double* ky;
     const double* kz;
@@ -106,6 +108,95 @@ __host__ __device__ constexpr int spass_tx(int L, int esz) {
     int tx = 128 / esz;
     while (tx > 1 && tx * T > 256) tx /= 2;
     return tx;
+}
+
+// Paired complex64 strided pass (k_spass2) tile, in pairs of x values.
+// Default tile: up to 16 pairs (32 x values, 256 bytes of a row) in a CTA of
+// at most 128 threads (8 pairs = 128 bytes for lines of 16 threads, 4 pairs
+// for 32).
+__host__ __device__ constexpr int spass2_txp(int L) {
+    const int T = L / make_plan(L).E;
+    int txp = 16;
+    while (txp > 1 && txp * T > 128) txp /= 2;
+    return txp;
+}
+
+// ---- strided-pass variants (the autotuner's search space) --------------------
+// A variant fixes the implementation of a one-field strided pass (scalar
+// lines, k_spass, or paired complex64 lines, k_spass2), its tile width (x
+// values, or pairs of x values, per CTA) and the resident CTAs per SM its
+// launch bounds ask for (which sets the register budget).  Variant 0 is the
+// default of each precision; the others exist for the tuned lengths
+// (GPE_TUNED_*) only and are picked per (grid, axis, pass mode) by
+// gpe_tune.  The CTA count of a pass against the SM's resident slots decides
+// how full its last wave is, so tile and occupancy are searched together.
+struct SVar {
+    int ok;      // 1 when the variant exists for this length and precision
+    int paired;  // 1: k_spass2 (complex64 only)
+    int tile;    // TX (scalar) or TXP (paired)
+    int mb;      // __launch_bounds__ min blocks
+    int pv;      // radix-order variant of the line FFT (make_plan), paired passes
+};
+constexpr int NSVAR = 12;
+
+// Default resident CTAs of the scalar strided pass (as pass_min_blocks /
+// spass_min_blocks in gpe_kernels_impl.cuh): words of line values per thread.
+__host__ __device__ constexpr int spass_mb_default(int esz, int L, int NF) {
+    const int w = esz / 8 * make_plan(L).E * NF;  // esz 8 (complex64) or 16 (complex128)
+    const int pm = w <= 8 ? 3 : (w <= 16 ? 2 : 1);
+    return pm == 3 ? 5 : pm;
+}
+// Default resident CTAs of the paired pass (register budget: the pair values
+// plus 48, or 64 for plans with 12 or more values per thread).
+__host__ __device__ constexpr int spass2_mb_default(int L, int NF, int txp, int pv = 0) {
+    const int E = make_plan(L, pv).E;
+    const int regs0 = E * 4 * NF + (E > 8 ? 64 : 48);
+    const int regs = regs0 < 64 ? 64 : regs0;
+    const int threads = (txp * (L / E) + 31) / 32 * 32;
+    const int b = 65536 / (threads * regs);
+    const int bw = 2048 / threads;
+    return b < 1 ? 1 : (b > bw ? bw : (b > 32 ? 32 : b));
+}
+__host__ __device__ constexpr SVar svar_make(int esz, int L, int paired, int tile, int mb, int pv = 0) {
+    const PlanSpec ps = make_plan(L, pv);
+    const int T = ps.ok ? L / ps.E : 0;
+    const int threads = tile * T;
+    const int wthreads = (threads + 31) / 32 * 32;
+    const bool ok = ps.ok && tile >= 1 && mb >= 1 && mb <= 32 && threads >= 1 &&
+                    threads <= (paired ? 512 : 256) && wthreads * mb <= 2048 && (!paired || esz == 8) &&
+                    (pv == 0 || paired) && 65536 / (wthreads * mb) >= 32;
+    return SVar{ok ? 1 : 0, paired, tile, mb, pv};
+}
+// esz: bytes per complex value (8: complex64, 16: complex128); NF = 1.
+__host__ __device__ constexpr SVar svar(int esz, int L, int v) {
+    const int tx = spass_tx(L, esz);
+    const int mb0 = spass_mb_default(esz, L, 1);
+    if (v == 0) return SVar{make_plan(L).ok ? 1 : 0, 0, tx, mb0, 0};
+    if (esz == 8) {
+        const int tp = spass2_txp(L);
+        switch (v) {
+            case 1: return svar_make(8, L, 1, tp, spass2_mb_default(L, 1, tp));
+            case 2: return svar_make(8, L, 1, tp, spass2_mb_default(L, 1, tp) + 1);
+            case 3: return svar_make(8, L, 1, tp, spass2_mb_default(L, 1, tp) + 2);
+            case 4: return svar_make(8, L, 1, tp / 2, spass2_mb_default(L, 1, tp / 2));
+            case 5: return svar_make(8, L, 1, tp / 2, spass2_mb_default(L, 1, tp / 2) + 2);
+            case 6: return svar_make(8, L, 1, tp * 2, spass2_mb_default(L, 1, tp * 2));
+            case 7: return svar_make(8, L, 1, tp * 2, spass2_mb_default(L, 1, tp * 2) + 1);
+            case 8: return svar_make(8, L, 0, tx / 2, mb0 * 2);
+            case 9: return svar_make(8, L, 0, tx, mb0 + 1);
+            case 10: return svar_make(8, L, 1, tp, spass2_mb_default(L, 1, tp, 1), 1);
+            case 11: return svar_make(8, L, 1, tp, spass2_mb_default(L, 1, tp, 2), 2);
+            default: return SVar{0, 0, 0, 0, 0};
+        }
+    }
+    switch (v) {
+        case 1: return svar_make(16, L, 0, tx, mb0 + 1);
+        case 2: return svar_make(16, L, 0, tx, mb0 + 2);
+        case 3: return svar_make(16, L, 0, tx / 2, mb0 * 2);
+        case 4: return svar_make(16, L, 0, tx / 2, mb0 * 2 + 2);
+        case 5: return svar_make(16, L, 0, tx * 2, mb0 > 1 ? mb0 / 2 : 1);
+        default: return SVar{0, 0, 0, 0, 0};
+    }
 }
 
 // ---- shared-memory line addressing -----------------------------------------

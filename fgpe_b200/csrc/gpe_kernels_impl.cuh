@@ -11,6 +11,8 @@
 // resident per SM, which is what hides the memory latency.
 #pragma once
 
+#include <atomic>
+
 #include "gpe_kernels.cuh"
 
 namespace gpe {
@@ -292,6 +294,7 @@ template <typename R, int EPI, int NF, int STG>
 __device__ __forceinline__ EpiIn<typename Cx<R>::T> load_inputs(const PassArgs<R>& a, const PsiScale<R>& ps,
                                                                 long long gi, int cur) {
     typedef typename Cx<R>::T C;
+    if constexpr (EPI == EPI_STORE) return EpiIn<C>{};  // the store epilogue reads no inputs
     EpiIn<C> in;
     const int nc = ncomp_of<NF>(a);
     const int stage = STG ? STG : a.stage;
@@ -671,14 +674,18 @@ __global__ void __launch_bounds__(256, (xpass_min_blocks<R, L, NF, KIND>())) k_x
     constexpr int RinF = Plan<L>::in_radix(false);
     constexpr int RoutF = Plan<L>::out_radix(false);
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    pass_prologue_sync();
     const InstPtr ip = select_instance(a);
     const long long boff = ip.boff;
-    if (a.check_done && ip.sc->done) return;
     if constexpr (KIND == XK_RKF || KIND == XK_RK || KIND == XK_RKO) {
+        // The epilogue inputs were written two or more launches earlier, so
+        // the L2 prefetch may run before the wait for the preceding grid
+        // (with programmatic launch this CTA can start during its tail);
+        // a prefetch is only a cache hint either way.
         const int nr = min(rows, a.nrows - (int)blockIdx.x * rows);
         if (nr > 0) prefetch_rk_inputs<R, NF>(a, boff + (long long)blockIdx.x * rows * L, nr, L);
     }
+    pass_prologue_sync();
+    if (a.check_done && ip.sc->done) return;
 
     C* X = reinterpret_cast<C*>(smem_raw);
     const unsigned b = threadIdx.x / T, t = threadIdx.x % T;
@@ -784,8 +791,11 @@ __host__ __device__ constexpr int spass_min_blocks() {
     return pass_min_blocks<R, L, NF>() == 3 ? 5 : pass_min_blocks<R, L, NF>();
 }
 
-template <typename R, int L, int NF>
-__global__ void __launch_bounds__(256, (spass_min_blocks<R, L, NF>())) k_spass(PassArgs<R> a, int ntx) {
+// TX: x values per CTA (tile width); MB: resident CTAs per SM the launch
+// bounds ask for.  The defaults are spass_tx and spass_min_blocks; other
+// (TX, MB) pairs are autotuner variants (gpe_tune.cu).
+template <typename R, int L, int NF, int TX, int MB>
+__global__ void __launch_bounds__(256, MB) k_spass(PassArgs<R> a, int ntx) {
     typedef typename Cx<R>::T C;
     constexpr int E = Plan<L>::E;
     constexpr int T = Plan<L>::T;
@@ -797,7 +807,7 @@ __global__ void __launch_bounds__(256, (spass_min_blocks<R, L, NF>())) k_spass(P
     if (a.check_done && (a.sc + (a.nbatch > 1 ? blockIdx.y : 0))->done) return;
 
     C* X = reinterpret_cast<C*>(smem_raw);
-    constexpr int tx = spass_tx(L, (int)sizeof(C));
+    constexpr int tx = TX;
     const int xb = blockIdx.x % ntx, outer = blockIdx.x / ntx;
     const int x0 = xb * tx;
     const unsigned b = threadIdx.x % tx, t = threadIdx.x / tx;
@@ -868,6 +878,144 @@ __global__ void __launch_bounds__(256, (spass_min_blocks<R, L, NF>())) k_spass(P
     }
 }
 
+// ---- paired complex64 strided pass ------------------------------------------------
+// k_spass for complex64 fields with an even nx, two lines per thread
+// (gpe_pair.cuh): one CTA = 2*TXP consecutive x values x the whole line for
+// one outer index; thread (b, t) = (pair b of the tile, thread t of the line),
+// b fast, so a quarter warp loads 8 pairs = 128 contiguous bytes of a line
+// position.  Shared memory: S[pos * TXP + b], 16-byte pair slots.
+// Default resident CTAs of a paired pass: spass2_mb_default (gpe_kernels.cuh).
+template <int L, int NF, int TXP>
+__host__ __device__ constexpr int spass2_min_blocks() {
+    return spass2_mb_default(L, NF, TXP);
+}
+
+template <int NF>
+__device__ __forceinline__ void spec_point2(const PassArgs<float>& a, cpair (&v)[NF], int ix, int iy, int iz,
+                                            long long gi) {
+    const int npsi = npsi_of<NF>(a);
+    if (a.spec == SPEC_PX) {  // v * kx per lane, in FP64 as the scalar pass
+        const double k0 = a.kx[ix], k1 = a.kx[ix + 1];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+            v[f].x.v = make_float2((float)(v[f].x.v.x * k0), (float)(v[f].x.v.y * k1));
+            v[f].y.v = make_float2((float)(v[f].y.v.x * k0), (float)(v[f].y.v.y * k1));
+        }
+        return;
+    }
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+        if (f < npsi) {
+            const double rl = a.rot[f < 2 ? f : 0];
+            f2x fac;
+            if (rl == 0.0) {
+                // (k2x + k2y) + k2z in float, lane by lane as the scalar pass
+                const f2x kxx{*reinterpret_cast<const float2*>(a.k2s[0] + ix)};
+                const float ky2 = a.k2s[1][iy], kz2 = a.k2s[2][iz];
+                fac = (kxx + f2x{make_float2(ky2, ky2)}) + f2x{make_float2(kz2, kz2)};
+            } else {
+                const double kyz = a.ky[iy] * a.ky[iy] + a.kz[iz] * a.kz[iz];
+                const double k0 = a.kx[ix], k1 = a.kx[ix + 1];
+                fac.v = make_float2((float)(a.lap_scale * (k0 * k0 + kyz) - k0 * rl),
+                                    (float)(a.lap_scale * (k1 * k1 + kyz) - k1 * rl));
+            }
+            v[f].x = v[f].x * fac;
+            v[f].y = v[f].y * fac;
+        } else {
+            const f2x d{*reinterpret_cast<const float2*>(a.vdd + gi)};
+            v[f].x = v[f].x * d;
+            v[f].y = v[f].y * d;
+        }
+    }
+}
+
+template <int L, int NF, int TXP, int MB, int PV>
+__global__ void __launch_bounds__(TXP * Plan<L, PV>::T, MB) k_spass2(PassArgs<float> a, int ntx) {
+    typedef Plan<L, PV> PL;
+    constexpr int E = PL::E;
+    constexpr int T = PL::T;
+    constexpr int RinF = PL::in_radix(false);
+    constexpr int RoutF = PL::out_radix(false);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    pass_prologue_sync();
+    const long long boff = select_instance(a).boff;
+    if (a.check_done && (a.sc + (a.nbatch > 1 ? blockIdx.y : 0))->done) return;
+
+    cpair* X = reinterpret_cast<cpair*>(smem_raw);
+    const int xb = blockIdx.x % ntx, outer = blockIdx.x / ntx;
+    const int x0 = xb * (2 * TXP);
+    const unsigned b = threadIdx.x % TXP, t = threadIdx.x / TXP;
+    const int xa = x0 + 2 * (int)b;
+    const bool valid = xa < a.nx;  // nx is even: a pair is whole or absent
+    const long long ss = a.sstride;
+    // g0 + reg_off(e) * ss: global index of the first value of register e's pair
+    const long long g0 = boff + (long long)outer * a.ostride + (valid ? xa : x0) + (long long)t * ss;
+    const ColAddr<cpair, TXP> addr{X + b};
+    const float4* tw = a.tw2;
+    const int mode = a.mode;
+    cpair v[NF][E];
+    const cpair zero{f2x{make_float2(0.f, 0.f)}, f2x{make_float2(0.f, 0.f)}};
+
+    if (mode == SM_INV) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const long long gi = g0 + (long long)reg_off<L, E, T, RoutF>(e) * ss;
+#pragma unroll
+            for (int f = 0; f < NF; ++f)
+                v[f][e] = valid ? pair_from(*reinterpret_cast<const float4*>(a.w[f] + gi)) : zero;
+        }
+#pragma unroll
+        for (int f = 0; f < NF; ++f) line_fft_inv<L, PV>(v[f], addr, tw, t);
+    } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const long long gi = g0 + (long long)reg_off<L, E, T, RinF>(e) * ss;
+#pragma unroll
+            for (int f = 0; f < NF; ++f)
+                v[f][e] = valid ? pair_from(*reinterpret_cast<const float4*>(a.w[f] + gi)) : zero;
+        }
+#pragma unroll
+        for (int f = 0; f < NF; ++f) line_fft_fwd<L, PV>(v[f], addr, tw, t);
+        if (mode == SM_FWD) {
+            if (valid) {
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const long long gi = g0 + (long long)reg_off<L, E, T, RoutF>(e) * ss;
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) *reinterpret_cast<float4*>(a.w[f] + gi) = pair_to(v[f][e]);
+                }
+            }
+            return;
+        }
+        if (a.spec != SPEC_NONE) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int pos = reg_pos<L, E, T, RoutF>((int)t, e);
+                cpair tmp[NF];
+#pragma unroll
+                for (int f = 0; f < NF; ++f) tmp[f] = v[f][e];
+                if (valid) {
+                    const int iy = (a.sax == 2) ? outer : pos;
+                    const int iz = (a.sax == 2) ? pos : outer;
+                    spec_point2<NF>(a, tmp, xa, iy, iz, g0 + (long long)reg_off<L, E, T, RoutF>(e) * ss);
+                }
+#pragma unroll
+                for (int f = 0; f < NF; ++f) v[f][e] = tmp[f];
+            }
+        }
+#pragma unroll
+        for (int f = 0; f < NF; ++f) line_fft_inv<L, PV>(v[f], addr, tw, t);
+    }
+    if (valid) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const long long gi = g0 + (long long)reg_off<L, E, T, RinF>(e) * ss;
+#pragma unroll
+            for (int f = 0; f < NF; ++f) *reinterpret_cast<float4*>(a.w[f] + gi) = pair_to(v[f][e]);
+        }
+    }
+}
+
 // ---- launchers ----------------------------------------------------------------------
 // rows: rows per CTA (x pass); smem: exchange buffer bytes; both chosen by the host.
 // Launch with programmatic stream serialization (see pass_prologue_sync).
@@ -888,18 +1036,26 @@ cudaError_t launch_pass(K kernel, unsigned grid, unsigned nbatch, unsigned threa
 }
 
 // Exchange buffers above the default 48 KB (short lines with E = 12..24
-// values per thread and 256 rows, complex128) need the opt-in attribute.
+// values per thread and 256 rows, complex128) need the opt-in attribute.  The
+// attribute belongs to one device, so it is recorded per device (bit d of
+// done_mask, devices 0..63; others set it on every launch), and the mask is
+// atomic because distinct handles may launch from different host threads.
 template <typename K>
-cudaError_t allow_smem(K kernel, size_t smem, bool& done) {
-    if (smem <= 48 * 1024 || done) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    if (e == cudaSuccess) done = true;
+cudaError_t allow_smem(K kernel, size_t smem, std::atomic<unsigned long long>& done_mask) {
+    if (smem <= 48 * 1024) return cudaSuccess;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = (dev >= 0 && dev < 64) ? (1ull << dev) : 0ull;
+    if (bit && (done_mask.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    if (e == cudaSuccess && bit) done_mask.fetch_or(bit, std::memory_order_acq_rel);
     return e;
 }
 
 template <typename R, int L, int NF, int KIND>
 cudaError_t launch_xpass_kind(const PassArgs<R>& a, int rows, size_t smem, cudaStream_t st) {
-    static bool attr = false;
+    static std::atomic<unsigned long long> attr{0};
     cudaError_t e = allow_smem(k_xpass<R, L, NF, KIND>, smem, attr);
     if (e != cudaSuccess) return e;
     const int threads = rows * Plan<L>::T;
@@ -944,17 +1100,71 @@ cudaError_t launch_xpass(const PassArgs<R>& a, int rows, size_t smem, cudaStream
     }
 }
 
-template <typename R, int L, int NF>
-cudaError_t launch_spass(const PassArgs<R>& a, int nouter, size_t smem, cudaStream_t st) {
-    static bool attr = false;
-    cudaError_t e = allow_smem(k_spass<R, L, NF>, smem, attr);
+// smem is recomputed here from the tile (the host passes the default's size).
+template <typename R, int L, int NF, int TX = spass_tx(L, (int)sizeof(typename Cx<R>::T)),
+          int MB = spass_min_blocks<R, L, NF>()>
+cudaError_t launch_spass(const PassArgs<R>& a, int nouter, size_t /*smem*/, cudaStream_t st) {
+    static std::atomic<unsigned long long> attr{0};
+    const size_t smem = (size_t)L * TX * sizeof(typename Cx<R>::T);
+    cudaError_t e = allow_smem(k_spass<R, L, NF, TX, MB>, smem, attr);
     if (e != cudaSuccess) return e;
-    constexpr int tx = spass_tx(L, (int)sizeof(typename Cx<R>::T));
-    const int threads = tx * Plan<L>::T;
-    const int ntx = (a.nx + tx - 1) / tx;
-    return launch_pass(k_spass<R, L, NF>, (unsigned)(ntx * nouter), (unsigned)a.nbatch, (unsigned)threads, smem, st,
-                       a, ntx);
+    const int threads = TX * Plan<L>::T;
+    const int ntx = (a.nx + TX - 1) / TX;
+    return launch_pass(k_spass<R, L, NF, TX, MB>, (unsigned)(ntx * nouter), (unsigned)a.nbatch, (unsigned)threads,
+                       smem, st, a, ntx);
 }
+
+template <int L, int NF, int TXP = spass2_txp(L), int MB = spass2_min_blocks<L, NF, TXP>(), int PV = 0>
+cudaError_t launch_spass2(const PassArgs<float>& a, int nouter, size_t /*smem*/, cudaStream_t st) {
+    static std::atomic<unsigned long long> attr{0};
+    const size_t smem = (size_t)L * TXP * sizeof(float4);
+    cudaError_t e = allow_smem(k_spass2<L, NF, TXP, MB, PV>, smem, attr);
+    if (e != cudaSuccess) return e;
+    const int threads = TXP * Plan<L, PV>::T;
+    const int ntx = (a.nx + 2 * TXP - 1) / (2 * TXP);
+    return launch_pass(k_spass2<L, NF, TXP, MB, PV>, (unsigned)(ntx * nouter), (unsigned)a.nbatch,
+                       (unsigned)threads, smem, st, a, ntx);
+}
+
+// Strided-pass variant V of length L, one field (svar in gpe_kernels.cuh).
+// *found is false when the variant does not exist for this length/precision.
+template <typename R, int L, int V>
+cudaError_t launch_svar_v(const PassArgs<R>& a, int nouter, cudaStream_t st, bool* found) {
+    constexpr SVar s = svar((int)sizeof(typename Cx<R>::T), L, V);
+    if constexpr (!s.ok) {
+        *found = false;
+        return cudaSuccess;
+    } else if constexpr (s.paired) {
+        if constexpr (sizeof(R) == 4) {
+            return launch_spass2<L, 1, s.tile, s.mb, s.pv>(a, nouter, 0, st);
+        } else {
+            *found = false;
+            return cudaSuccess;
+        }
+    } else {
+        return launch_spass<R, L, 1, s.tile, s.mb>(a, nouter, 0, st);
+    }
+}
+template <typename R, int L>
+cudaError_t launch_svar(int v, const PassArgs<R>& a, int nouter, cudaStream_t st, bool* found) {
+    *found = true;
+    switch (v) {
+        case 0: return launch_svar_v<R, L, 0>(a, nouter, st, found);
+        case 1: return launch_svar_v<R, L, 1>(a, nouter, st, found);
+        case 2: return launch_svar_v<R, L, 2>(a, nouter, st, found);
+        case 3: return launch_svar_v<R, L, 3>(a, nouter, st, found);
+        case 4: return launch_svar_v<R, L, 4>(a, nouter, st, found);
+        case 5: return launch_svar_v<R, L, 5>(a, nouter, st, found);
+        case 6: return launch_svar_v<R, L, 6>(a, nouter, st, found);
+        case 7: return launch_svar_v<R, L, 7>(a, nouter, st, found);
+        case 8: return launch_svar_v<R, L, 8>(a, nouter, st, found);
+        case 9: return launch_svar_v<R, L, 9>(a, nouter, st, found);
+        case 10: return launch_svar_v<R, L, 10>(a, nouter, st, found);
+        case 11: return launch_svar_v<R, L, 11>(a, nouter, st, found);
+        default: *found = false; return cudaSuccess;
+    }
+}
+static_assert(NSVAR == 12, "launch_svar lists every variant");
 
 // Threads per line for a length (host side).
 inline int plan_threads(int L) { return L / make_plan(L).E; }

@@ -19,7 +19,10 @@
 //    current: it looks up the scratch's device address (which may also load
 //    this file's kernel onto the device) and zeroes the completion counter
 //    with a synchronous cudaMemset.  Make that first call before any stream
-//    capture begins on the device.
+//    capture begins on the device.  The address is cached per device for
+//    the life of the process; cudaDeviceReset on a device leaves the cached
+//    address pointing into the destroyed context, so the entry point must not
+//    be called on that device again in the same process.
 //  - What must start at zero: the completion counter in the first bytes of the
 //    scratch.  It is zero when the module loads, the set-up zeroes it again,
 //    and the last block of every call puts it back to zero.  The block

@@ -289,8 +289,15 @@ FILE* open_or_throw(const std::string& fn, const char* mode) {
 }
 }  // namespace
 
-// src/output.cu:26-90 (ly/lz use NX[0], as the reference writes them)
+// src/output.cu:26-90.  The reference writes ly and lz with NX[0]
+// (src/output.cu:42-44); that stays the default, so downstream readers see
+// the same file.  The optional input key `wtxt_ref_lengths false` writes
+// ly = NX[1] DX[1] aho and lz = NX[2] DX[2] aho instead.
 void Output::WriteWtxt(const Params& p, int ncycle) {
+    const bool ref_lengths =
+        p.getIV().getVariable("wtxt_ref_lengths") == "None" || p.getBool("wtxt_ref_lengths");
+    const int ny_l = ref_lengths ? p.NX[0] : p.NX[1];
+    const int nz_l = ref_lengths ? p.NX[0] : p.NX[2];
     FILE* file = open_or_throw(prefix + "info.wtxt", "w");
     fprintf(file, "cycles                   %d\n\n", ncycle);
     fprintf(file, "dim                      %d\n", p.DIM);
@@ -301,8 +308,8 @@ void Output::WriteWtxt(const Params& p, int ncycle) {
     fprintf(file, "dy                       %lf\n", p.DX[1]);
     fprintf(file, "dz                       %lf\n", p.DX[2]);
     fprintf(file, "lx                       %lf\n", p.NX[0] * p.DX[0] * p.aho);
-    fprintf(file, "ly                       %lf\n", p.NX[0] * p.DX[1] * p.aho);
-    fprintf(file, "lz                       %lf\n", p.NX[0] * p.DX[2] * p.aho);
+    fprintf(file, "ly                       %lf\n", ny_l * p.DX[1] * p.aho);
+    fprintf(file, "lz                       %lf\n", nz_l * p.DX[2] * p.aho);
     fprintf(file, "datadim                  %d\n", 3);
     fprintf(file, "prefix                   %s\n", p.outpath.c_str());
     fprintf(file, "t0                       %lf\n", p.time0);

@@ -61,8 +61,9 @@ typedef enum gpe_status {
  *            sum at the last stage), so its rounding does not accumulate;
  *            gpe_set_psi stores the complex128 input's rounding residual as
  *            the low part and gpe_get_psi returns the sum.  Imaginary-time
- *            steps, gpe_fft and the control gradient use the high part
- *            alone and drop the low part. */
+ *            steps and gpe_fft use the high part alone and drop the low
+ *            part; the control gradient carries both parts through its
+ *            forward steps and checkpoints. */
 typedef enum gpe_precision { GPE_C128 = 0, GPE_C64 = 1 } gpe_precision;
 
 /* Which Hamiltonian plugin supplies the pointwise term.
@@ -74,7 +75,9 @@ typedef enum gpe_precision { GPE_C128 = 0, GPE_C64 = 1 } gpe_precision;
  *                   real-space cut-off radius R (0 = no cut-off).  The kernel
  *                   is 12*pi*a_dd*((k.d)^2/k^2 - 1/3) as in
  *                   src/parallel.cu:326-352 (never called there), times
- *                   1 + 3cos(kR)/(kR)^2 - 3sin(kR)/(kR)^3 with k in rad/length.
+ *                   1 + 3cos(kR)/(kR)^2 - 3sin(kR)/(kR)^3 with k in rad/length
+ *                   (summed as its power series below kR = 0.5, where the
+ *                   closed form cancels; 0 at k = 0, the limit).
  *  GPE_HAM_SOFT     one component, h = T + (V + Phi) psi with the mean field
  *                   Phi = IFFT(V~(k) FFT|psi|^2) / N of a soft-core
  *                   interaction, V~ of SoftCoreInteraction_1D/2D/3D
@@ -138,6 +141,16 @@ gpe_status  gpe_config_init(gpe_config* cfg);
 /* 1 when a grid length has a device FFT plan (products of 2, 3 and 5 up to
  * 1024 whose plan needs at most 24 values per thread), else 0. */
 int         gpe_fft_length_supported(int n);
+/* The k-space interaction kernel V~(k) that gpe_create uploads for
+ * GPE_HAM_DIPOLAR or GPE_HAM_SOFT (documented with gpe_hamiltonian), before
+ * the division by the number of points that the unnormalised inverse
+ * transform needs: out[iz*NY*NX + iy*NX + ix] at the k axes of
+ * BaseHamiltonian::InitializeKspace (src/baseHamiltonian.cu:53-82), FP64,
+ * NX*NY*NZ values.  Host arithmetic only (no device is touched).  The dipolar
+ * form is the reference's DipoleDipoleInteraction (src/parallel.cu:326-352)
+ * times the spherical cut-off factor; the soft-core forms are
+ * SoftCoreInteraction_1D/2D/3D (src/parallel.cu:360-477). */
+gpe_status  gpe_kspace_kernel(const gpe_config* cfg, double* out);
 
 /* ---- lifecycle: replaces Cuda::Cuda / ~Cuda (src/parallel.cu:14-113,
  * hpp/parallel.hpp:80-126) and BaseHamiltonian::InitializeKspace/Space
@@ -286,12 +299,51 @@ long long  gpe_batch_kernel_launches(const gpe_batch* b);
  * implies.  n above GPE_NORM_NOALLOC_MAX_POINTS is rejected with
  * GPE_ERR_UNSUPPORTED.  The first call on each device does a one-time set-up
  * (scratch address lookup, a synchronous zeroing of its completion counter):
- * make it before any stream capture starts on that device.  Calls that may
- * overlap on one device share the scratch and race; order them on one stream.
- * The result is the same bits on every call for the same input. */
+ * make it before any stream capture starts on that device.  The scratch
+ * address found there is kept for the life of the process: after
+ * cudaDeviceReset on a device it would point into the destroyed context, so
+ * do not call this entry point on that device again in the same process.
+ * Calls that may overlap on one device share the scratch and race; order
+ * them on one stream.  The result is the same bits on every call for the
+ * same input. */
 #define GPE_NORM_NOALLOC_MAX_POINTS 134217728LL /* 512^3 */
 gpe_status gpe_norm_noalloc(const void* dev_psi_c128, long long n, double dv, double* dev_out,
                             void* cuda_stream);
+
+/* ---- autotuner (no counterpart in the reference, which leaves the transform
+ * plan to cuFFT's planner, cufftPlan1d/2d/3d at src/parallel.cu:77-110) -----
+ * The pass kernels come in variants: per strided axis and pass mode
+ * (forward, forward*k-space*inverse, inverse) the implementation (scalar
+ * lines, or two complex64 lines per thread with packed FP32x2 arithmetic),
+ * the tile width, the resident CTAs per SM and the radix order of the line
+ * FFT; per grid the x pass's rows per CTA.  Variant 0 / rows 0 are the
+ * defaults, which every handle uses unless a tuning result applies.
+ *
+ * gpe_tune times every variant that exists for cfg's grid (CUDA events on a
+ * temporary handle: each strided pass alone, the rows by whole steps of the
+ * workload, 0 = real-time RK4 steps, 1 = imaginary-time iterations), keeps
+ * the fastest, and stores one line keyed by (nx, ny, nz, precision, fields,
+ * instances = 1) in the JSON-lines file cache_path (replacing a line of the
+ * same key; NULL = do not store).  report (may be NULL) receives 10 values:
+ * default and tuned microseconds per step, variants timed, the chosen
+ * variants s[axis 1][mode 0..2], s[axis 2][mode 0..2], and the rows. */
+gpe_status gpe_tune(const gpe_config* cfg, int workload, const char* cache_path, double* report);
+/* Process-wide: gpe_create and gpe_batch_create apply the cache line that
+ * matches a new handle (or batch group); NULL = read $GPE_TUNE_CACHE if set. */
+gpe_status gpe_set_tune_cache(const char* path);
+/* Tunes every geometry group of a batch in place (imaginary-time
+ * iterations with the group's instance count), drops its captured graph, and
+ * stores a line per group in cache_path (may be NULL).  report (may be NULL):
+ * 2 values per group, default and tuned microseconds per iteration. */
+gpe_status gpe_batch_tune(gpe_batch* b, const char* cache_path, double* report);
+int        gpe_batch_groups(const gpe_batch* b);
+/* The handle's variants as 7 ints: s[1][0..2], s[2][0..2], rows.  Setting
+ * checks that each variant exists (gpe_pass_variant_exists) for the grid. */
+gpe_status gpe_get_pass_variants(const gpe_handle* h, int* out7);
+gpe_status gpe_set_pass_variants(gpe_handle* h, const int* in7);
+/* 1 when strided-pass variant v (0 .. 11) exists for axis 1 (y) or 2 (z) of
+ * cfg's grid, precision and fields; variant 0 always does.  Host only. */
+int        gpe_pass_variant_exists(const gpe_config* cfg, int axis, int v);
 
 /* Synchronise the handle's stream and report any asynchronous error. */
 gpe_status gpe_sync(gpe_handle* h);

@@ -259,6 +259,21 @@ struct orc_solver {
         build_vdd();
     }
 
+    // Spherical cut-off factor c(q) = 1 + 3cos(q)/q^2 - 3sin(q)/q^3
+    // = 3 int_0^q j2(x)/x dx; for q < 0.5, where the closed form cancels, the
+    // power series 3 sum_n (-1)^n q^(2n+2) / ((2n+2) 2^n n! (2n+5)!!).
+    static double cutoff_factor(double q) {
+        if (q >= 0.5) return 1.0 + 3.0 * std::cos(q) / (q * q) - 3.0 * std::sin(q) / (q * q * q);
+        double sum = 0.0;
+        for (int n = 0; n < 8; ++n) {
+            double den = 2.0 * n + 2.0;
+            for (int i = 1; i <= n; ++i) den *= 2.0 * i;       // 2^n n!
+            for (int i = 1; i <= 2 * n + 5; i += 2) den *= i;  // (2n+5)!!
+            sum += ((n % 2) ? -1.0 : 1.0) * std::pow(q, 2 * n + 2) / den;
+        }
+        return 3.0 * sum;
+    }
+
     // Dipolar kernel 12 pi a_dd ((k.d)^2/k^2 - 1/3), src/parallel.cu:326-352
     // (0 for |k| < 1e-6 as there), times the spherical cut-off factor
     // 1 + 3cos(q)/q^2 - 3sin(q)/q^3, q = 2 pi |k| R (its q -> 0 limit is 0).
@@ -286,7 +301,7 @@ struct orc_solver {
                         v = 12.0 * PI_REF * add * ((num / den) * (num / den) - 1.0 / 3.0);
                         if (R > 0) {
                             double q = 2.0 * PI_REF * den * R;
-                            v *= 1.0 + 3.0 * std::cos(q) / (q * q) - 3.0 * std::sin(q) / (q * q * q);
+                            v *= cutoff_factor(q);
                         }
                     }
                     vdd[idx] = v;

@@ -14,7 +14,9 @@
 #                        full-precision PARS).  Needs a GPU.
 # The reference's own Makefile passes no -arch; here every object is built for
 # sm_100a with the reference's other flags (-std=c++20 -O3).
-REF   ?= /root/reference
+# the reference's source tree: REF=..., else $GPE_REFERENCE_DIR, else /root/reference
+GPE_REFERENCE_DIR ?= /root/reference
+REF   ?= $(GPE_REFERENCE_DIR)
 HERE  := $(dir $(abspath $(lastword $(MAKEFILE_LIST))))
 OUT   := $(HERE)_ref
 OBJ   := $(OUT)/obj

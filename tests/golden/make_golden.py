@@ -22,6 +22,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.dirname(HERE))
+import golden_util as gu  # noqa: E402
 REF_TRACE = os.path.join(ROOT, "oracle", "_ref", "gpe_ref_trace")
 REF_STOCK = os.path.join(ROOT, "oracle", "_ref", "gpe_ref")
 
@@ -37,6 +40,7 @@ CASES = [
     ("g_stock_rt", REF_STOCK, 1),
     ("g_stock_rot", REF_STOCK, 1),
     ("g_stock_rot_rt", REF_STOCK, 1),
+    ("g_cfg1_hb64", REF_TRACE, 1),
 ]
 
 
@@ -75,6 +79,15 @@ def main():
         inp = os.path.join(work, case + ".txt")
         with open(inp, "w") as f:
             f.write(src.replace("@OUT@", work + "/"))
+        generated = None
+        if case in gu.GENERATED:
+            # the trap and the seeded initial state, as the .wdat files the input reads
+            _, o = gu.params_dump(src, work)
+            psi, V = gu.cfg1_inputs(o)
+            keys = gu.keys(src.replace("@OUT@", work + "/"))
+            psi.astype(np.complex128).tofile(keys["inprefix"].strip('"') + "psi_final.wdat")
+            V.astype(np.complex128).tofile(keys["vprefix"].strip('"') + "vext.wdat")
+            generated = gu.input_checksums(psi, V)
         r = subprocess.run([binary, inp], capture_output=True, text=True, timeout=600)
         with open(os.path.join(work, case + ".log"), "w") as f:
             f.write(r.stdout + "\n---stderr---\n" + r.stderr)
@@ -83,7 +96,16 @@ def main():
             sys.exit(1)
         pre = os.path.join(work, case + "_")
         d = {"input": np.array(src), "ncomp": np.array(nc), "stdout": np.array(r.stdout)}
-        if nc == 1:
+        if generated is not None:
+            # the reference wrote back the state and trap it read
+            for name, arr in (("psi_init.wdat", psi), ("vext.wdat", V)):
+                got = read_c128(pre + name)
+                if got.size and not np.array_equal(got, arr):
+                    print(f"{case}: {name} differs from the generated input", file=sys.stderr)
+                    sys.exit(1)
+            d.update(generated)
+            d["psi_final"] = read_c128(pre + "psi_final.wdat")
+        elif nc == 1:
             d["psi_init"] = read_c128(pre + "psi_init.wdat")
             d["vext"] = read_c128(pre + "vext.wdat")
             d["psi_final"] = read_c128(pre + "psi_final.wdat")

@@ -9,18 +9,68 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
-TRACE_CASES = ["g_hb_bec", "g_hb_conv", "g_rt_quench", "g_hb_bec2", "g_rt_bec2", "g_hb_template"]
+TRACE_CASES = ["g_hb_bec", "g_hb_conv", "g_rt_quench", "g_hb_bec2", "g_rt_bec2", "g_hb_template", "g_cfg1_hb64"]
 STOCK_CASES = ["g_stock_2d", "g_stock_rt", "g_stock_rot", "g_stock_rot_rt"]
 # real-time stock cases start from the psi_final of an imaginary-time case
 PREREQ = {"g_stock_rt": "g_stock_2d", "g_stock_rot_rt": "g_stock_rot"}
+
+
+# Cases whose initial state and trap are regenerated from a seed instead of
+# being stored (their inputs would be most of the fixture): the fixture keeps
+# checksums of the inputs the reference read, and load() checks them.
+GENERATED = ["g_cfg1_hb64"]
 
 
 def available(case):
     return os.path.exists(os.path.join(GOLDEN, case + ".npz"))
 
 
+def cfg1_inputs(o):
+    """Config 1 inputs on the grid of the parameter dump o (gpeh_params):
+    V = (x^2 + y^2 + z^2)/2 and psi0 = exp(-r^2/2) (1 + 1e-3 (n1 + i n2)) with
+    n1, n2 standard normal from numpy's legacy RandomState(1) (a frozen
+    stream), normalised to 1.  Cell-centred axes x_i = -XMAX + (i + 1/2) DX
+    (src/baseHamiltonian.cu:25-51)."""
+    n = [int(o[0]), int(o[1]), int(o[2])]
+    ax = [-o[5 + d] + np.arange(n[d]) * o[8 + d] + 0.5 * o[8 + d] for d in range(3)]
+    Z, Y, X = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+    r2 = X * X + Y * Y + Z * Z
+    V = (0.5 * r2 + 0j).reshape(-1)
+    rng = np.random.RandomState(1)
+    n1 = rng.standard_normal(r2.shape)
+    n2 = rng.standard_normal(r2.shape)
+    psi = np.exp(-r2 / 2.0) * (1.0 + 1e-3 * (n1 + 1j * n2))
+    dv = o[8] * o[9] * o[10]
+    psi = psi / np.sqrt(np.sum(np.abs(psi) ** 2) * dv)
+    return psi.reshape(-1), V
+
+
+def input_checksums(psi, V):
+    """Norms and leading values of the regenerated inputs."""
+    return {"psi_init_norm2": np.array(np.sum(np.abs(psi) ** 2)), "psi_init_head": psi[:1024].copy(),
+            "vext_norm2": np.array(np.sum(np.abs(V) ** 2)), "vext_head": V[:1024].copy()}
+
+
+def regenerate(fx, tmpdir=None):
+    """psi_init and vext of a GENERATED case, checked against the checksums
+    stored with the fixture (to 1e-14: the arrays come from libm exp, which
+    may differ in the last bit between hosts)."""
+    import tempfile
+    d = tmpdir or tempfile.mkdtemp()
+    _, o = params_dump(str(fx["input"]), d)
+    psi, V = cfg1_inputs(o)
+    want = input_checksums(psi, V)
+    for k, v in want.items():
+        ref = fx[k]
+        assert np.max(np.abs(v - ref)) <= 1e-14 * max(np.max(np.abs(ref)), 1e-300), k
+    return psi, V
+
+
 def load(case):
-    return dict(np.load(os.path.join(GOLDEN, case + ".npz"), allow_pickle=False))
+    fx = dict(np.load(os.path.join(GOLDEN, case + ".npz"), allow_pickle=False))
+    if case in GENERATED and "psi_init" not in fx:
+        fx["psi_init"], fx["vext"] = regenerate(fx)
+    return fx
 
 
 def keys(text):

@@ -26,6 +26,9 @@ def test_round_trip_and_parseval(gpu, prec, tol, shape):
         s.set_psi(0, a)
         s.fft(0, -1)
         f = s.get_psi(0)
+        # the spectrum itself (a consistently permuted or mis-twiddled
+        # spectrum would pass the round trip and Parseval below)
+        assert rel(f, np.fft.fftn(a)) < 10 * tol
         # Parseval for the unnormalised transform
         assert abs(np.sum(np.abs(f) ** 2) / (a.size * np.sum(np.abs(a) ** 2)) - 1) < 10 * tol
         s.fft(0, +1)

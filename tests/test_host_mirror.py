@@ -122,6 +122,34 @@ def test_info_wtxt_identical(case, tmp_path):
     assert info.read_bytes() == want
 
 
+def test_info_wtxt_lengths_key(tmp_path):
+    """ly/lz of info.wtxt: NX[0]*DX[1]*aho and NX[0]*DX[2]*aho as the reference
+    writes them (src/output.cu:42-44) unless `wtxt_ref_lengths false`."""
+    names = (ctypes.c_char_p * 1)(b"en")
+    units = (ctypes.c_char_p * 1)(b"code")
+    vals = np.array([1.0])
+    lines = {}
+    for flag in (None, "true", "false"):
+        src = open(os.path.join(INPUTS, "bec_harmonic_3d.txt")).read().replace("@OUT@", str(tmp_path) + "/run_")
+        if flag is not None:
+            src += f"\nwtxt_ref_lengths {flag}\n"
+        fn = tmp_path / "in.txt"
+        fn.write_text(src)
+        assert ours().gpeh_write_info(str(fn).encode(), 1, 1, names, dp(vals), units) == 0
+        txt = (tmp_path / "run_info.wtxt").read_text()
+        lines[flag] = {l.split()[0]: float(l.split()[1]) for l in txt.splitlines()
+                       if l.split() and l.split()[0] in ("nx", "ny", "nz", "dx", "dy", "dz", "lx", "ly", "lz")}
+    assert lines[None] == lines["true"]
+    d = lines["false"]
+    p = np.zeros(47)
+    assert ours().gpeh_params(str(tmp_path / "in.txt").encode(), dp(p)) == 1
+    aho = p[24]
+    for ax, n, DX in (("ly", "ny", p[9]), ("lz", "nz", p[10])):
+        assert d[n] != d["nx"]
+        assert abs(d[ax] - d[n] * DX * aho) < 1e-5 * max(1.0, d[ax])
+        assert abs(lines[None][ax] - d["nx"] * DX * aho) < 1e-5 * max(1.0, d[ax])
+
+
 def test_missing_key_is_an_error_not_exit(tmp_path):
     src = open(os.path.join(INPUTS, "bec_2d.txt")).read().replace("@OUT@", str(tmp_path) + "/run_")
     src = "\n".join(l for l in src.splitlines() if not l.startswith("mass"))

@@ -72,3 +72,38 @@ def test_norm_noalloc_rejects_bad_arguments(gpu):
     assert f(buf.data_ptr(), -1, 1.0, out.data_ptr(), st) == 1
     assert f(buf.data_ptr() + 8, 4, 1.0, out.data_ptr(), st) == 1  # not 16-byte aligned
     assert f(buf.data_ptr(), 4, 1.0, None, st) == 1
+
+
+def test_norm_noalloc_first_call_on_a_side_stream(gpu, tmp_path):
+    """The one-time set-up of a device (scratch address lookup and a
+    synchronous zeroing of the completion counter) must also be right when
+    the very first call of the process is issued on a non-default stream:
+    run that first call in a fresh process."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    prog = (
+        "import ctypes, numpy as np, torch, sys\n"
+        f"sys.path.insert(0, {root!r})\n"
+        "from fgpe_b200 import lib\n"
+        "f = lib().gpe_norm_noalloc\n"
+        "f.restype = ctypes.c_int\n"
+        "f.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]\n"
+        "rng = np.random.default_rng(3)\n"
+        "a = rng.standard_normal(300000) + 1j * rng.standard_normal(300000)\n"
+        "d = torch.from_numpy(a).to('cuda')\n"
+        "out = torch.full((2,), float('nan'), dtype=torch.float64, device='cuda')\n"
+        "s = torch.cuda.Stream()\n"
+        "torch.cuda.synchronize()\n"
+        "with torch.cuda.stream(s):\n"
+        "    assert f(d.data_ptr(), a.size, 0.5, out.data_ptr(), s.cuda_stream) == 0\n"
+        "    assert f(d.data_ptr(), a.size, 0.5, out.data_ptr() + 8, s.cuda_stream) == 0\n"
+        "s.synchronize()\n"
+        "got = out.cpu().numpy()\n"
+        "want = np.sum(np.abs(a) ** 2) * 0.5\n"
+        "assert abs(got[0] - want) <= 1e-12 * want and got[0] == got[1], (got, want)\n"
+        "print('ok')\n"
+    )
+    r = subprocess.run([sys.executable, "-c", prog], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
