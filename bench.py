@@ -64,6 +64,8 @@ def parse():
     p.add_argument("--fd-components", type=int, default=32, help="control2d: finite-difference checks")
     p.add_argument("--sweep-instances", type=int, default=256)
     p.add_argument("--no-tune", action="store_true", help="keep the default pass variants (no autotuning)")
+    p.add_argument("--tune-cache", default=None,
+                   help="JSON-lines tuning cache to reuse: grids with a line there are not tuned again")
     p.add_argument("--sweep-converge", action="store_true",
                    help="sweep2d: also run every instance to |dmu| < 1e-8 and report the iterations")
     return p.parse_args()
@@ -102,6 +104,24 @@ def initial_psi(cfg, seed=1):
     psi = g * (1 + 1e-3 * (rng.standard_normal(g.shape) + 1j * rng.standard_normal(g.shape)))
     dv = cfg.dx[0] * cfg.dx[1] * cfg.dx[2]
     return psi / np.sqrt(np.sum(np.abs(psi) ** 2) * dv)
+
+
+def cached_or_tune(cfg, workload, cache):
+    """The cache's line for cfg's grid (nb = 1), or a fresh tuning stored there."""
+    import fgpe_b200 as gp
+    if os.path.exists(cache):
+        nf = cfg.ncomp + (1 if cfg.hamiltonian in (gp.HAM_DIPOLAR, gp.HAM_SOFT) else 0)
+        for line in open(cache):
+            try:
+                d = json.loads(line)
+            except ValueError:
+                continue
+            if (d.get("nx"), d.get("ny"), d.get("nz"), d.get("prec"), d.get("nf"), d.get("nb")) == \
+                    (cfg.nx, cfg.ny, cfg.nz, cfg.precision, nf, 1):
+                return {"default_us": d["default_us"], "tuned_us": d["tuned_us"], "from_cache": cache,
+                        "variants": [d[k] for k in ("s10", "s11", "s12", "s20", "s21", "s22")],
+                        "xrows": d["xrows"], "yz": d.get("yz", 0)}
+    return gp.tune(cfg, workload, cache)
 
 
 def workload_conf(n, world=1):
@@ -222,11 +242,11 @@ def run_ours(args):
 
     # autotune the pass variants of both forms for this grid (setup, like a
     # transform planner: outside the timed region), then create the handles
-    tune_cache = os.path.join("/tmp", f"gpe_tune_{os.getpid()}.jsonl")
+    tune_cache = args.tune_cache or os.path.join("/tmp", f"gpe_tune_{os.getpid()}.jsonl")
     tuning = {}
     if not args.no_tune:
         for name, prec in (("c64", gp.C64), ("c128", gp.C128)):
-            tuning[name] = gp.tune(workload_config(n, prec, G1), 0, tune_cache)
+            tuning[name] = cached_or_tune(workload_config(n, prec, G1), 0, tune_cache)
         gp.set_tune_cache(tune_cache)
     solvers = {}
     for name, prec in (("c64", gp.C64), ("c128", gp.C128)):
@@ -770,6 +790,12 @@ def run_control(args):
     s.close()
     target = X.reshape(psi0.shape) * np.abs(psi0)
     target = target / np.sqrt(np.sum(np.abs(target) ** 2) * dv) + 0j
+    tuning = {}
+    if not args.no_tune:
+        cache = os.path.join("/tmp", f"gpe_tune_{os.getpid()}.jsonl")
+        for name, cfg in (("c64", cfg64), ("c128", cfgg)):
+            tuning[name] = gp.tune(cfg, 0, cache)
+        gp.set_tune_cache(cache)
     solvers = {}
     for name, cfg in (("c64", cfg64), ("c128", cfgg)):
         sv = gp.Solver(cfg)
@@ -793,19 +819,25 @@ def run_control(args):
     t0 = time.perf_counter()
     s64.control_gradient(u, target, 50, want_grad=False)
     fwd = time.perf_counter() - t0
-    # finite differences of the complex128 forward map
+    # finite differences of the complex128 forward map: the fourth-order
+    # central stencil (-L(u+2h) + 8 L(u+h) - 8 L(u-h) + L(u-2h)) / 12h, whose
+    # truncation error (h^4) stays far below the 1e-4 bar; the second-order
+    # stencil's h^2 L''' term alone reaches ~5e-5 on this nearly degenerate
+    # loss (L ~ 1 - 3e-7)
     rng = np.random.default_rng(7)
     h = 1e-4
     s128 = solvers["c128"]
     L128, g128 = s128.control_gradient(u, target, 50)
     errs = []
+
+    def loss_at(n, k, d):
+        uu = u.copy()
+        uu[n, k] += d
+        return s128.control_gradient(uu, target, 50, want_grad=False)[0]
+
     for _ in range(args.fd_components):
         n, k = rng.integers(u.shape[0]), rng.integers(u.shape[1])
-        up, um = u.copy(), u.copy()
-        up[n, k] += h
-        um[n, k] -= h
-        fd = (s128.control_gradient(up, target, 50, want_grad=False)[0]
-              - s128.control_gradient(um, target, 50, want_grad=False)[0]) / (2 * h)
+        fd = (-loss_at(n, k, 2 * h) + 8 * loss_at(n, k, h) - 8 * loss_at(n, k, -h) + loss_at(n, k, -2 * h)) / (12 * h)
         errs.append((abs(grad[n, k] - fd), abs(fd), abs(g128[n, k] - fd)))
     gmax = float(np.abs(g128).max())
     big = [e / f for e, f, _ in errs if f > 1e-2 * gmax]
@@ -821,14 +853,39 @@ def run_control(args):
             "loss_c64": L, "loss_c128": L128, "forward_only_s": round(fwd, 4),
             "gradient_s": round(wall, 4), "rk4_step_equivalents_per_s": round(u.shape[0] / wall, 1),
             "grad_rel_l2_c64_vs_c128": float(np.linalg.norm(grad - g128) / np.linalg.norm(g128)),
-            "fd": {"components": len(errs), "h": h, "fd_of": "complex128 forward",
+            "fd": {"components": len(errs), "h": h, "fd_of": "complex128 forward", "stencil": "4th-order central",
                    "max_rel_err_components_above_1pct_of_max": max(big) if big else None,
                    "max_abs_err_over_max_grad": max(e for e, _, _ in errs) / gmax,
                    "complex128_adjoint_max_rel_err": max(big128) if big128 else None},
-            "ground_state_iterations": int(gs_iters), "gpu_launches_per_gradient": int(launches)}
+            "ground_state_iterations": int(gs_iters), "gpu_launches_per_gradient": int(launches),
+            "tuning": tuning or "off (--no-tune): default pass variants"}
     for sv in solvers.values():
         sv.close()
+    if not args.quick:
+        line["cpu_baseline"] = control_cpu_leg(cfgg, V0, G, psi0, target, u, grad, g128)
     print(json.dumps(line))
+
+
+def control_cpu_leg(cfg, V0, G, psi0, target, u, grad64, grad128):
+    """CPU leg of the control workload: the FP64 numpy restatement of the
+    controlled RK4 step and its discrete adjoint (oracle/adjoint_oracle.py),
+    timed for one full gradient (2000 steps x 16 controls at 256^2), and, as
+    the checker, both GPU gradients against it."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import adjoint_oracle as ad
+    o = ad.ControlProblem(cfg, V0, G, psi0, target)
+    t0 = time.perf_counter()
+    Lo, go = o.gradient(u)
+    dt = time.perf_counter() - t0
+    nrm = float(np.linalg.norm(go))
+    gmax = float(np.abs(go).max())
+    big = np.abs(go) > 1e-2 * gmax
+    return {"value": round(1.0 / dt, 5), "unit": "gradients/s", "cores": 1, "kind": "port",
+            "sample": "one full gradient in FP64 numpy (oracle/adjoint_oracle.py)", "loss": float(Lo),
+            "parity_vs_port": {"grad_rel_l2_c128": float(np.linalg.norm(grad128 - go) / nrm),
+                               "grad_rel_l2_c64": float(np.linalg.norm(grad64 - go) / nrm),
+                               "max_rel_err_c64_components_above_1pct_of_max":
+                                   float(np.max(np.abs(grad64 - go)[big] / np.abs(go)[big]))}}
 
 
 def imag_case(name, precision, scheme):

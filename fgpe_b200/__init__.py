@@ -29,7 +29,7 @@ LIB_PATH = os.path.join(HERE, "libgpe.so")
 
 NO_HAMIL_PARAMS = 32
 C128, C64 = 0, 1
-HAM_BEC, HAM_BEC2, HAM_TEMPLATE, HAM_DIPOLAR, HAM_SOFT = 0, 1, 2, 3, 4
+HAM_BEC, HAM_BEC2, HAM_TEMPLATE, HAM_DIPOLAR, HAM_SOFT, HAM_USER = 0, 1, 2, 3, 4, 5
 IMAG_HEAVYBALL, IMAG_RK4 = 0, 1
 ABI_VERSION = 1
 
@@ -124,6 +124,7 @@ def lib() -> ctypes.CDLL:
         "gpe_get_pass_variants": (c_int, [H, POINTER(c_int)]),
         "gpe_set_pass_variants": (c_int, [H, POINTER(c_int)]),
         "gpe_pass_variant_exists": (c_int, [POINTER(GPEConfig), c_int, c_int]),
+        "gpe_set_user_hamiltonian": (c_int, [H, c_void_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -198,10 +199,10 @@ def tune(cfg: GPEConfig, workload: int = 0, cache_path: str | None = None) -> di
     """Autotune the pass variants of cfg's grid (gpe_tune): workload 0 =
     real-time RK4 steps, 1 = imaginary-time iterations.  Stores the result
     in the JSON-lines cache_path when given."""
-    rep = np.zeros(10)
+    rep = np.zeros(11)
     _check(lib().gpe_tune(byref(cfg), workload, cache_path.encode() if cache_path else None, _dp(rep)))
     return {"default_us": float(rep[0]), "tuned_us": float(rep[1]), "timed": int(rep[2]),
-            "variants": [int(x) for x in rep[3:9]], "xrows": int(rep[9])}
+            "variants": [int(x) for x in rep[3:9]], "xrows": int(rep[9]), "yz": int(rep[10])}
 
 
 def set_tune_cache(path: str | None) -> None:
@@ -383,14 +384,20 @@ class Solver:
 
     PROF_KINDS = ("x_fwd", "x_inv", "x_full", "s_fwd", "s_inv", "s_fki")
 
+    def set_user_hamiltonian(self, ops_ptr: int) -> None:
+        """Install a user Hamiltonian plugin (the gpe_user_hamiltonian table a
+        plugin built with include/gpe_plugin.cuh returns) on a HAM_USER handle."""
+        _check(lib().gpe_set_user_hamiltonian(self.handle, c_void_p(ops_ptr)))
+
     def pass_variants(self) -> list:
-        """[s(y, fwd), s(y, fki), s(y, inv), s(z, fwd), s(z, fki), s(z, inv), x rows]."""
-        out = (c_int * 7)()
+        """[s(y, fwd), s(y, fki), s(y, inv), s(z, fwd), s(z, fki), s(z, inv), x rows, fused y-z]."""
+        out = (c_int * 8)()
         _check(lib().gpe_get_pass_variants(self.handle, out))
         return list(out)
 
     def set_pass_variants(self, v) -> None:
-        arr = (c_int * 7)(*[int(x) for x in v])
+        v = list(v) + [0] * (8 - len(v))
+        arr = (c_int * 8)(*[int(x) for x in v])
         _check(lib().gpe_set_pass_variants(self.handle, arr))
 
     def profile(self, enable: bool) -> None:

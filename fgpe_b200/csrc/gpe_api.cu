@@ -51,6 +51,8 @@ int plan_T(int L) { return L / make_plan(L).E; }
 
 enum StateMode { ST_CANON = 0, ST_HB = 1, ST_RKI = 2 };
 
+constexpr int YZ_XB_HOST = 4;  // x values per slab of the fused y-z kernel (YZ_XB, gpe_yz.cuh)
+
 }  // namespace
 
 // Lets other translation units of the library (gpe_noalloc.cu) record the
@@ -81,6 +83,11 @@ struct gpe_handle {
     // xrows = rows per CTA of the x passes (0 = default)
     int svar[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     int xrows = 0;
+    // user Hamiltonian plugin (GPE_HAM_USER, gpe_set_user_hamiltonian)
+    const gpe_user_hamiltonian* user = nullptr;
+    // 1: the strided part of a 3D complex64 stage runs as the fused y-z
+    // cluster kernel (k_yz, gpe_yz.cuh) where the grid allows it
+    int yz = 0;
     double* kax[3] = {nullptr, nullptr, nullptr};
     float* k2s[3] = {nullptr, nullptr, nullptr};  // complex64: lap_scale * k^2 per axis
     double* obs_part = nullptr;                    // OBS_BLOCKS partial sums + the result
@@ -437,6 +444,7 @@ PassArgs<R> base_args(gpe_handle* h) {
         a.vext[c] = (const C*)h->V[c];
         a.pin[c] = (const C*)h->A[c];
     }
+    a.twz = nullptr;
     a.kx = h->kax[0];
     a.ky = h->kax[1];
     a.kz = h->kax[2];
@@ -516,8 +524,18 @@ gpe_status launch_x(gpe_handle* h, PassArgs<R> a, int nf, int mode) {
     if (h->xrows > 0 && h->xrows < rows) rows = h->xrows;
     const size_t smem = (size_t)rows * xpad(L) * sizeof(C);
     cudaError_t err = cudaSuccess;
-    if (!dispatch_x(L, nf, a, rows, smem, h->st, &err))
+    if (a.ham == GPE_HAM_USER && mode != XM_FWD && a.epi != EPI_STORE) {
+        // the passes that evaluate the Hamiltonian run the user plugin's kernels
+        if (!h->user) return fail(GPE_ERR_INVALID_ARG, "GPE_HAM_USER handle without gpe_set_user_hamiltonian");
+        int e = 0;
+        const int found = sizeof(R) == 4 ? h->user->launch_x_c64(L, &a, rows, smem, (void*)h->st, &e)
+                                         : h->user->launch_x_c128(L, &a, rows, smem, (void*)h->st, &e);
+        if (!found)
+            return fail(GPE_ERR_UNSUPPORTED, "the user Hamiltonian plugin has no kernel for length " + std::to_string(L));
+        err = (cudaError_t)e;
+    } else if (!dispatch_x(L, nf, a, rows, smem, h->st, &err)) {
         return fail(GPE_ERR_UNSUPPORTED, "no x-pass kernel for length " + std::to_string(L));
+    }
     if (err != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("x pass launch: ") + cudaGetErrorString(err));
     h->launches++;
     return GPE_OK;
@@ -572,6 +590,32 @@ gpe_status launch_s(gpe_handle* h, PassArgs<R> a, int nf, int axis, int mode) {
 // last strided axis forward * k-space * inverse, strided inverse passes,
 // x-inverse with epilogue.  a.pro / a.epi / a.stage ... are set by the caller.
 // skip_fwd: W already holds the x-forward transform of the stage input.
+// Whether the fused y-z cluster kernel can serve a chain of nf fields.
+bool yz_usable(const gpe_handle* h, int nf) {
+    return h->prec == GPE_C64 && nf == 1 && h->ny > 1 && h->nz > 1 && h->nx % YZ_XB_HOST == 0 &&
+           yz_shape_supported(h->ny, h->nz);
+}
+
+// The fused y-z kernel in place of the three strided passes (profiled as
+// pass kind 5).
+template <typename R>
+gpe_status launch_yz_chain(gpe_handle* h, PassArgs<R> a) {
+    if constexpr (sizeof(R) == 4) {
+        ProfScope ps(h, 5);
+        a.tw = (const float2*)h->tw[1];
+        a.twz = (const float2*)h->tw[2];
+        cudaError_t err = cudaSuccess;
+        if (!dispatch_yz(h->ny, h->nz, a, h->st, &err))
+            return fail(GPE_ERR_UNSUPPORTED, "no fused y-z kernel for this grid");
+        if (err != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("y-z kernel launch: ") + cudaGetErrorString(err));
+        h->launches++;
+        return GPE_OK;
+    } else {
+        (void)a;
+        return fail(GPE_ERR_UNSUPPORTED, "the fused y-z kernel is complex64 only");
+    }
+}
+
 template <typename R>
 gpe_status run_chain(gpe_handle* h, const PassArgs<R>& a, int nf, bool skip_fwd = false) {
     int axes[2], na = 0;
@@ -579,6 +623,10 @@ gpe_status run_chain(gpe_handle* h, const PassArgs<R>& a, int nf, bool skip_fwd 
     if (h->nz > 1) axes[na++] = 2;
     if (na == 0) return launch_x<R>(h, a, nf, XM_FULL);
     if (!skip_fwd) GPE_TRY(launch_x<R>(h, a, nf, XM_FWD));
+    if (h->yz && yz_usable(h, nf)) {
+        GPE_TRY(launch_yz_chain<R>(h, a));
+        return launch_x<R>(h, a, nf, XM_INV);
+    }
     for (int i = 0; i < na - 1; ++i) GPE_TRY(launch_s<R>(h, a, nf, axes[i], SM_FWD));
     GPE_TRY(launch_s<R>(h, a, nf, axes[na - 1], SM_FKI));
     for (int i = na - 2; i >= 0; --i) GPE_TRY(launch_s<R>(h, a, nf, axes[i], SM_INV));
@@ -1214,7 +1262,7 @@ gpe_status create_handle(const gpe_config* cfg, int nb, gpe_handle** out) {
     if (cfg->nx < 1 || cfg->ny < 1 || cfg->nz < 1) return fail(GPE_ERR_INVALID_ARG, "grid sizes must be >= 1");
     if (cfg->ncomp < 1 || cfg->ncomp > 2) return fail(GPE_ERR_INVALID_ARG, "ncomp must be 1 or 2");
     if (cfg->precision != GPE_C128 && cfg->precision != GPE_C64) return fail(GPE_ERR_INVALID_ARG, "bad precision");
-    if (cfg->hamiltonian < GPE_HAM_BEC || cfg->hamiltonian > GPE_HAM_SOFT)
+    if (cfg->hamiltonian < GPE_HAM_BEC || cfg->hamiltonian > GPE_HAM_USER)
         return fail(GPE_ERR_INVALID_ARG, "bad hamiltonian");
     if (cfg->ncomp == 2 && cfg->hamiltonian != GPE_HAM_BEC2 && cfg->hamiltonian != GPE_HAM_TEMPLATE)
         return fail(GPE_ERR_UNSUPPORTED, "two components need GPE_HAM_BEC2 or GPE_HAM_TEMPLATE");
@@ -1597,6 +1645,15 @@ gpe_status gpe_fft(gpe_handle* h, int comp, int sign) {
     if (sign != -1 && sign != 1) return fail(GPE_ERR_INVALID_ARG, "sign must be -1 or +1");
     GPE_TRY(h->prec == GPE_C64 ? fft_t<float>(h, comp, sign) : fft_t<double>(h, comp, sign));
     return check_device_status(h);
+}
+
+gpe_status gpe_set_user_hamiltonian(gpe_handle* h, const gpe_user_hamiltonian* ops) {
+    GPE_TRY(check_handle(h));
+    if (h->cfg.hamiltonian != GPE_HAM_USER) return fail(GPE_ERR_INVALID_ARG, "the handle's hamiltonian is not GPE_HAM_USER");
+    if (!ops || ops->abi_version != GPE_ABI_VERSION || !ops->launch_x_c64 || !ops->launch_x_c128)
+        return fail(GPE_ERR_INVALID_ARG, "null plugin table or abi_version mismatch");
+    h->user = ops;
+    return GPE_OK;
 }
 
 gpe_status gpe_sync(gpe_handle* h) {
@@ -2013,7 +2070,7 @@ std::string tune_line(const gpe_handle* h, double def_us, double tuned_us) {
       << ",\"nf\":" << k.nf << ",\"nb\":" << k.nb;
     for (int ax = 1; ax <= 2; ++ax)
         for (int m = 0; m < 3; ++m) o << ",\"s" << ax << m << "\":" << h->svar[ax][m];
-    o << ",\"xrows\":" << h->xrows;
+    o << ",\"xrows\":" << h->xrows << ",\"yz\":" << h->yz;
     char buf[64];
     std::snprintf(buf, sizeof(buf), ",\"default_us\":%.3f,\"tuned_us\":%.3f}", def_us, tuned_us);
     o << buf;
@@ -2042,6 +2099,8 @@ void tune_apply_cache(gpe_handle* h) {
         }
     int r = 0;
     if (json_int(hit, "xrows", &r) && r >= 0 && r <= 256) h->xrows = r;
+    int yz = 0;
+    if (json_int(hit, "yz", &yz) && (yz == 0 || (yz == 1 && yz_usable(h, h->nf)))) h->yz = yz;
 }
 
 // Replaces the line of h's key in the cache file (or appends it).
@@ -2198,6 +2257,18 @@ gpe_status tune_handle_t(gpe_handle* h, int workload, double* report) {
         }
     }
     h->xrows = best_r;
+    // the fused y-z cluster kernel against the chosen strided passes
+    if (yz_usable(h, h->nf)) {
+        h->yz = 1;
+        double us = 0.0;
+        gpe_status s = time_steps<R>(h, workload, &us);
+        ++timed;
+        if (s != GPE_OK || !(us < best_us * 0.99)) {
+            cudaGetLastError();
+            h->yz = 0;
+        }
+        GPE_CUDA(cudaStreamSynchronize(h->st));
+    }
     double tuned_us = 0.0;
     GPE_TRY(time_steps<R>(h, workload, &tuned_us));
     if (report) {
@@ -2218,6 +2289,7 @@ gpe_status tune_config(const gpe_config* cfg, int nb, int workload, double* repo
     for (int ax = 0; ax < 3; ++ax)
         for (int m = 0; m < 3; ++m) h->svar[ax][m] = 0;
     h->xrows = 0;
+    h->yz = 0;
     gpe_status s = h->prec == GPE_C64 ? tune_handle_t<float>(h, workload, report)
                                       : tune_handle_t<double>(h, workload, report);
     if (s != GPE_OK) {
@@ -2255,6 +2327,7 @@ gpe_status gpe_tune(const gpe_config* cfg, int workload, const char* cache_path,
         for (int ax = 1; ax <= 2; ++ax)
             for (int m = 0; m < 3; ++m) report[3 + (ax - 1) * 3 + m] = h->svar[ax][m];
         report[9] = h->xrows;
+        report[10] = h->yz;
     }
     cudaStreamSynchronize(h->st);
     free_all(h);
@@ -2267,6 +2340,7 @@ gpe_status gpe_get_pass_variants(const gpe_handle* h, int* out) {
     for (int ax = 1; ax <= 2; ++ax)
         for (int m = 0; m < 3; ++m) out[(ax - 1) * 3 + m] = h->svar[ax][m];
     out[6] = h->xrows;
+    out[7] = h->yz;
     return GPE_OK;
 }
 
@@ -2278,9 +2352,12 @@ gpe_status gpe_set_pass_variants(gpe_handle* h, const int* in) {
                 return fail(GPE_ERR_UNSUPPORTED, "pass variant " + std::to_string(in[(ax - 1) * 3 + m]) +
                                                      " does not exist for axis " + std::to_string(ax));
     if (in[6] < 0 || in[6] > 256) return fail(GPE_ERR_INVALID_ARG, "xrows must be 0..256");
+    if (in[7] != 0 && !(in[7] == 1 && yz_usable(h, h->nf)))
+        return fail(GPE_ERR_UNSUPPORTED, "the fused y-z kernel does not serve this grid");
     for (int ax = 1; ax <= 2; ++ax)
         for (int m = 0; m < 3; ++m) h->svar[ax][m] = in[(ax - 1) * 3 + m];
     h->xrows = in[6];
+    h->yz = in[7];
     return GPE_OK;
 }
 
@@ -2307,6 +2384,7 @@ gpe_status gpe_batch_tune(gpe_batch* b, const char* cache_path, double* report) 
         for (int ax = 0; ax < 3; ++ax)
             for (int m = 0; m < 3; ++m) hg->svar[ax][m] = t->svar[ax][m];
         hg->xrows = t->xrows;
+        hg->yz = t->yz;
         gpe_status s = tune_store(t, cache_path, rep[0], rep[1]);
         cudaStreamSynchronize(t->st);
         free_all(t);

@@ -65,6 +65,10 @@ inline bool dispatch_sv(int L, int v, const PassArgs<double>& a, int nouter, cud
     return false;
 }
 
+// Fused y-z cluster kernel of a 3D complex64 stage (gpe_yz.cu).
+bool yz_shape_supported(int ly, int lz);
+bool dispatch_yz(int ly, int lz, const PassArgs<float>& a, cudaStream_t st, cudaError_t* err);
+
 // Paired complex64 strided pass (needs an even nx; see k_spass2).
 inline bool dispatch_s2(int L, int NF, const PassArgs<float>& a, int nouter, size_t smem, cudaStream_t st,
                         cudaError_t* err) {

@@ -82,6 +82,7 @@ struct PassArgs {
     C* out[4];               // EPI_APPLYH: h_mu c0, h_en c0, h_mu c1, h_en c1
     const C* tw;             // roots of unity for this pass's length
     const float4* tw2;       // complex64: the same roots as (cos, cos, sin, sin) for the paired passes
+    const C* twz;            // fused y-z kernel: roots of unity of the z length (tw holds y's)
     const double* kx;
     const double* ky;
     const double* kz;

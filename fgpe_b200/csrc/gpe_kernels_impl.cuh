@@ -275,6 +275,55 @@ __device__ void reduce_and_finalize(const PassArgs<R>& a, const InstPtr& ip, DD 
     }
 }
 
+// ---- Hamiltonian policies ------------------------------------------------------------
+// The x-inverse epilogues evaluate the pointwise Hamiltonian through a policy
+// type H: coef() builds, once per CTA, what the pointwise term needs from
+// d_h_params and the time; point() evaluates h_mu (and h_en) at one grid
+// point.  BuiltinHam is the library's plugins (ham_point); UserHam<U> adapts
+// a user functor compiled in the user's own translation unit
+// (include/gpe_plugin.cuh), the counterpart of the reference's user-written
+// Hamiltonian kernels (hamiltonians/BEC_oneComponent.hpp:8-22,
+// hamiltonians/single_template.cu:333-373).
+struct BuiltinHam {
+    template <typename R> using Coef = HamCoef<R>;
+    static constexpr bool builtin = true;
+    template <typename R>
+    __device__ __forceinline__ static HamCoef<R> coef(const PassArgs<R>& a, const double* prms) {
+        return make_coef<R>(a, prms);
+    }
+    template <typename R, typename C, int MC>
+    __device__ __forceinline__ static void point(const PassArgs<R>& a, int nc, const HamCoef<R>& hc, const C* psi,
+                                                 const C* T, const C* V, R phi, bool want_en, C* hmu, C* hen) {
+        ham_point<R, C, MC>(a.ham, nc, hc, psi, T, V, phi, want_en, hmu, hen);
+    }
+};
+
+// U provides (one component, R = float or double, C = float2 or double2):
+//   template <typename R> struct Coef { ... };
+//   template <typename R> __device__ static Coef<R> coef(const double* prms, double t);
+//   template <typename R, typename C> __device__ static void point(const Coef<R>& k, C psi, C T, C V,
+//                                                                   bool want_en, C& hmu, C& hen);
+// with T the kinetic part (the reference's KEpsi) at the point.
+template <class U>
+struct UserHam {
+    template <typename R> using Coef = typename U::template Coef<R>;
+    static constexpr bool builtin = false;
+    template <typename R>
+    __device__ __forceinline__ static Coef<R> coef(const PassArgs<R>& a, const double* prms) {
+        return U::template coef<R>(prms, a.t);
+    }
+    template <typename R, typename C, int MC>
+    __device__ __forceinline__ static void point(const PassArgs<R>& a, int nc, const Coef<R>& hc, const C* psi,
+                                                 const C* T, const C* V, R phi, bool want_en, C* hmu, C* hen) {
+        (void)a;
+        (void)nc;
+        (void)phi;
+        C e = T[0];
+        U::template point<R, C>(hc, psi[0], T[0], V[0], want_en, hmu[0], e);
+        if (want_en) hen[0] = e;
+    }
+};
+
 // ---- epilogue for one grid point ------------------------------------------------
 // The epilogue of a chunk of points first loads every input it needs
 // (load_inputs), then computes and stores (epilogue_point).  Loading first
@@ -294,54 +343,58 @@ template <typename R, int EPI, int NF, int STG>
 __device__ __forceinline__ EpiIn<typename Cx<R>::T> load_inputs(const PassArgs<R>& a, const PsiScale<R>& ps,
                                                                 long long gi, int cur) {
     typedef typename Cx<R>::T C;
-    if constexpr (EPI == EPI_STORE) return EpiIn<C>{};  // the store epilogue reads no inputs
-    EpiIn<C> in;
-    const int nc = ncomp_of<NF>(a);
-    const int stage = STG ? STG : a.stage;
-    if constexpr (EPI != EPI_STORE) {
+    if constexpr (EPI == EPI_STORE) {
+        return EpiIn<C>{};  // the store epilogue reads no inputs
+    } else {
+        EpiIn<C> in;
+        const int nc = ncomp_of<NF>(a);
+        const int stage = STG ? STG : a.stage;
+        if constexpr (EPI != EPI_STORE) {
 #pragma unroll
-        for (int c = 0; c < maxc_of<NF>(); ++c) {
-            if (c >= nc) continue;
-            in.V[c] = a.vext[c][gi];
-            if constexpr (EPI == EPI_RK) {
-                in.psi[c] = a.pin[c][gi];
-                if (stage > 1) {
-                    in.k[c] = a.kacc[c][gi];
-                    in.p0[c] = a.buf[0][c][gi];
-                }
-                if constexpr (sizeof(R) == 4)
-                    if (stage == 4 && a.lo[0] != nullptr) in.xo[c] = a.lo[c][gi];
-            } else if constexpr (EPI == EPI_HB) {
-                in.psi[c] = scaled(a.buf[cur][c][gi], ps.cur[c]);
-                in.xo[c] = a.buf[1 - cur][c][gi];
-            } else if constexpr (EPI == EPI_RKI) {
-                in.p0[c] = a.buf[0][c][gi];
-                if (stage > 1) {
+            for (int c = 0; c < maxc_of<NF>(); ++c) {
+                if (c >= nc) continue;
+                in.V[c] = a.vext[c][gi];
+                if constexpr (EPI == EPI_RK) {
                     in.psi[c] = a.pin[c][gi];
-                    in.k[c] = a.kacc[c][gi];
+                    if (stage > 1) {
+                        in.k[c] = a.kacc[c][gi];
+                        in.p0[c] = a.buf[0][c][gi];
+                    }
+                    if constexpr (sizeof(R) == 4)
+                        if (stage == 4 && a.lo[0] != nullptr) in.xo[c] = a.lo[c][gi];
+                } else if constexpr (EPI == EPI_HB) {
+                    in.psi[c] = scaled(a.buf[cur][c][gi], ps.cur[c]);
+                    in.xo[c] = a.buf[1 - cur][c][gi];
+                } else if constexpr (EPI == EPI_RKI) {
+                    in.p0[c] = a.buf[0][c][gi];
+                    if (stage > 1) {
+                        in.psi[c] = a.pin[c][gi];
+                        in.k[c] = a.kacc[c][gi];
+                    }
+                } else if constexpr (EPI == EPI_ADJ) {
+                    in.psi[c] = a.pin[c][gi];     // mu, the stage adjoint being applied
+                    in.p0[c] = a.buf[0][c][gi];   // psi_s, the stage argument
+                    in.k[c] = a.out[0][gi];       // lambda_{n+1}
+                    if (stage < 4) {
+                        in.xo[c] = a.kacc[c][gi];  // running sum of J^T terms
+                        in.aux = mk(reinterpret_cast<const R*>(a.out[1])[gi], (R)0);
+                    }
+                } else {
+                    in.psi[c] = load_psi<R>(a, ps, c, gi, cur);
                 }
-            } else if constexpr (EPI == EPI_ADJ) {
-                in.psi[c] = a.pin[c][gi];     // mu, the stage adjoint being applied
-                in.p0[c] = a.buf[0][c][gi];   // psi_s, the stage argument
-                in.k[c] = a.out[0][gi];       // lambda_{n+1}
-                if (stage < 4) {
-                    in.xo[c] = a.kacc[c][gi];  // running sum of J^T terms
-                    in.aux = mk(reinterpret_cast<const R*>(a.out[1])[gi], (R)0);
-                }
-            } else {
-                in.psi[c] = load_psi<R>(a, ps, c, gi, cur);
             }
         }
+        return in;
     }
-    return in;
 }
 
 // v: the NF inverse-transformed fields at global index gi (kinetic part per
 // psi component, dipolar potential field last); in: the loaded inputs.
 // For EPI_RK, nv receives the new state of each component (the value stored
 // in buf[1] for stages 1-3, in buf[0] for stage 4).
-template <typename R, int NF, int EPI, bool MAYRED, int STG>
-__device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const HamCoef<R>& hc, const PsiScale<R>& ps,
+template <typename R, int NF, int EPI, bool MAYRED, int STG, class H = BuiltinHam>
+__device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const typename H::template Coef<R>& hc,
+                                               const PsiScale<R>& ps,
                                                const typename Cx<R>::T* v, const EpiIn<typename Cx<R>::T>& in,
                                                long long gi, int cur, DD* acc, typename Cx<R>::T* nv) {
     typedef typename Cx<R>::T C;
@@ -367,7 +420,7 @@ __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const HamCo
 #pragma unroll
             for (int c = 0; c < MC; ++c)
                 if (c < nc) psi[c] = in.psi[c];
-            ham_point<R, C, MC>(a.ham, nc, hc, psi, T, V, phi, want_en, hmu, hen);
+            H::template point<R, C, MC>(a, nc, hc, psi, T, V, phi, want_en, hmu, hen);
             const R cr = (R)a.c_re, ci = (R)a.c_im;
 #pragma unroll
             for (int c = 0; c < MC; ++c) {
@@ -411,7 +464,7 @@ __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const HamCo
 #pragma unroll
             for (int c = 0; c < MC; ++c)
                 if (c < nc) psi[c] = in.psi[c];
-            ham_point<R, C, MC>(a.ham, nc, hc, psi, T, V, phi, true, hmu, hen);
+            H::template point<R, C, MC>(a, nc, hc, psi, T, V, phi, true, hmu, hen);
 #pragma unroll
             for (int c = 0; c < MC; ++c) {
                 if (c >= nc) continue;
@@ -444,7 +497,7 @@ __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const HamCo
                 p0[c] = make_double2((double)x.x * s, (double)x.y * s);
                 psi[c] = (stage == 1) ? from_d<C>(p0[c]) : in.psi[c];
             }
-            ham_point<R, C, MC>(a.ham, nc, hc, psi, T, V, phi, stage == 1, hmu, hen);
+            H::template point<R, C, MC>(a, nc, hc, psi, T, V, phi, stage == 1, hmu, hen);
 #pragma unroll
             for (int c = 0; c < MC; ++c) {
                 if (c >= nc) continue;
@@ -512,7 +565,7 @@ __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const HamCo
 #pragma unroll
             for (int c = 0; c < 2; ++c)
                 if (c < nc) psi[c] = in.psi[c];
-            ham_point<R, C, MC>(a.ham, nc, hc, psi, T, V, phi, true, hmu, hen);
+            H::template point<R, C, MC>(a, nc, hc, psi, T, V, phi, true, hmu, hen);
             if constexpr (EPI == EPI_APPLYH) {
 #pragma unroll
                 for (int c = 0; c < 2; ++c) {
@@ -543,8 +596,10 @@ __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const HamCo
 // register budget of the launch bounds holds without spilling.
 // FUSE: v[f][e] is replaced by the new RK state of component f (and, for the
 // dipolar density field, its |psi|^2), ready for the forward x transform.
-template <typename R, int NF, int EPI, bool MAYRED, int L, int E, int T, int Rr, bool FUSE = false, int STG = 0>
-__device__ __forceinline__ void epilogue_line(const PassArgs<R>& a, const HamCoef<R>& hc, const PsiScale<R>& ps,
+template <typename R, int NF, int EPI, bool MAYRED, int L, int E, int T, int Rr, bool FUSE = false, int STG = 0,
+          class H = BuiltinHam>
+__device__ __forceinline__ void epilogue_line(const PassArgs<R>& a, const typename H::template Coef<R>& hc,
+                                              const PsiScale<R>& ps,
                                               typename Cx<R>::T (&v)[NF][E], long long g0, int cur, DD* acc) {
     typedef typename Cx<R>::T C;
     constexpr bool LO = EPI == EPI_RK && sizeof(R) == 4 && (STG == 4 || STG == 0);  // may read the low part
@@ -562,7 +617,7 @@ __device__ __forceinline__ void epilogue_line(const PassArgs<R>& a, const HamCoe
 #pragma unroll
             for (int f = 0; f < NF; ++f) tmp[f] = v[f][e0 + j];
             C nv[2];
-            epilogue_point<R, NF, EPI, MAYRED, STG>(a, hc, ps, tmp, in[j], g0 + reg_off<L, E, T, Rr>(e0 + j), cur,
+            epilogue_point<R, NF, EPI, MAYRED, STG, H>(a, hc, ps, tmp, in[j], g0 + reg_off<L, E, T, Rr>(e0 + j), cur,
                                                     acc, nv);
             if constexpr (FUSE) {
                 const int npsi = npsi_of<NF>(a);
@@ -577,19 +632,20 @@ __device__ __forceinline__ void epilogue_line(const PassArgs<R>& a, const HamCoe
 }
 
 // Epilogue of a line with the op of the kernel role.
-template <typename R, int NF, int KIND, int L, int E, int T, int Rr>
-__device__ __forceinline__ void epilogue_dispatch(const PassArgs<R>& a, const HamCoef<R>& hc, const PsiScale<R>& ps,
+template <typename R, int NF, int KIND, int L, int E, int T, int Rr, class H = BuiltinHam>
+__device__ __forceinline__ void epilogue_dispatch(const PassArgs<R>& a, const typename H::template Coef<R>& hc,
+                                                  const PsiScale<R>& ps,
                                                   typename Cx<R>::T (&v)[NF][E], long long g0, int cur, DD* acc) {
-#define GPE_EPI(OP, RED) epilogue_line<R, NF, OP, RED, L, E, T, Rr>(a, hc, ps, v, g0, cur, acc)
+#define GPE_EPI(OP, RED) epilogue_line<R, NF, OP, RED, L, E, T, Rr, false, 0, H>(a, hc, ps, v, g0, cur, acc)
     if constexpr (KIND == XK_STORE) GPE_EPI(EPI_STORE, false);
     else if constexpr (KIND == XK_RK) GPE_EPI(EPI_RK, false);
     else if constexpr (KIND == XK_RKF) {
         // the hot real-time kernel: one copy of the epilogue per stage class
-        if (a.stage == 1) epilogue_line<R, NF, EPI_RK, false, L, E, T, Rr, true, 1>(a, hc, ps, v, g0, cur, acc);
-        else if (a.stage < 4) epilogue_line<R, NF, EPI_RK, false, L, E, T, Rr, true, 2>(a, hc, ps, v, g0, cur, acc);
-        else epilogue_line<R, NF, EPI_RK, false, L, E, T, Rr, true, 4>(a, hc, ps, v, g0, cur, acc);
+        if (a.stage == 1) epilogue_line<R, NF, EPI_RK, false, L, E, T, Rr, true, 1, H>(a, hc, ps, v, g0, cur, acc);
+        else if (a.stage < 4) epilogue_line<R, NF, EPI_RK, false, L, E, T, Rr, true, 2, H>(a, hc, ps, v, g0, cur, acc);
+        else epilogue_line<R, NF, EPI_RK, false, L, E, T, Rr, true, 4, H>(a, hc, ps, v, g0, cur, acc);
     } else if constexpr (KIND == XK_RKO) {  // launched for stage 4 only
-        epilogue_line<R, NF, EPI_RK, true, L, E, T, Rr, false, 4>(a, hc, ps, v, g0, cur, acc);
+        epilogue_line<R, NF, EPI_RK, true, L, E, T, Rr, false, 4, H>(a, hc, ps, v, g0, cur, acc);
     }
     else if constexpr (KIND == XK_HB) GPE_EPI(EPI_HB, true);
     else if constexpr (KIND == XK_RKI) GPE_EPI(EPI_RKI, true);
@@ -666,7 +722,7 @@ __device__ __forceinline__ void prefetch_rk_inputs(const PassArgs<R>& a, long lo
     }
 }
 
-template <typename R, int L, int NF, int KIND>
+template <typename R, int L, int NF, int KIND, class H = BuiltinHam>
 __global__ void __launch_bounds__(256, (xpass_min_blocks<R, L, NF, KIND>())) k_xpass(PassArgs<R> a, int rows) {
     typedef typename Cx<R>::T C;
     constexpr int E = Plan<L>::E;
@@ -752,10 +808,10 @@ __global__ void __launch_bounds__(256, (xpass_min_blocks<R, L, NF, KIND>())) k_x
         }
     }
     if constexpr (KIND != XK_FWD) {
-        const HamCoef<R> hc = make_coef<R>(a, ip.prms);
+        const typename H::template Coef<R> hc = H::template coef<R>(a, ip.prms);
 #pragma unroll
         for (int f = 0; f < NF; ++f) line_fft_inv<L>(v[f], addr, a.tw, t);
-        if (valid) epilogue_dispatch<R, NF, KIND, L, E, T, RinF>(a, hc, ps, v, g0, cur, acc);
+        if (valid) epilogue_dispatch<R, NF, KIND, L, E, T, RinF, H>(a, hc, ps, v, g0, cur, acc);
         if constexpr (KIND == XK_RKF) {
             // next stage's x-forward pass on the state just written (in place on w)
 #pragma unroll
@@ -795,7 +851,7 @@ __host__ __device__ constexpr int spass_min_blocks() {
 // bounds ask for.  The defaults are spass_tx and spass_min_blocks; other
 // (TX, MB) pairs are autotuner variants (gpe_tune.cu).
 template <typename R, int L, int NF, int TX, int MB>
-__global__ void __launch_bounds__(256, MB) k_spass(PassArgs<R> a, int ntx) {
+__global__ void __launch_bounds__(TX * Plan<L>::T, MB) k_spass(PassArgs<R> a, int ntx) {
     typedef typename Cx<R>::T C;
     constexpr int E = Plan<L>::E;
     constexpr int T = Plan<L>::T;
@@ -1053,14 +1109,14 @@ cudaError_t allow_smem(K kernel, size_t smem, std::atomic<unsigned long long>& d
     return e;
 }
 
-template <typename R, int L, int NF, int KIND>
+template <typename R, int L, int NF, int KIND, class H = BuiltinHam>
 cudaError_t launch_xpass_kind(const PassArgs<R>& a, int rows, size_t smem, cudaStream_t st) {
     static std::atomic<unsigned long long> attr{0};
-    cudaError_t e = allow_smem(k_xpass<R, L, NF, KIND>, smem, attr);
+    cudaError_t e = allow_smem(k_xpass<R, L, NF, KIND, H>, smem, attr);
     if (e != cudaSuccess) return e;
     const int threads = rows * Plan<L>::T;
     const int grid = (a.nrows + rows - 1) / rows;
-    return launch_pass(k_xpass<R, L, NF, KIND>, (unsigned)grid, (unsigned)a.nbatch, (unsigned)threads, smem, st, a,
+    return launch_pass(k_xpass<R, L, NF, KIND, H>, (unsigned)grid, (unsigned)a.nbatch, (unsigned)threads, smem, st, a,
                        rows);
 }
 
@@ -1078,25 +1134,27 @@ __host__ __device__ inline int xkind_of(int mode, int epi) {
     }
 }
 
-template <typename R, int L, int NF>
+// H: the Hamiltonian policy (BuiltinHam for the library's plugins; a user
+// plugin instantiates UserHam<U>, which has no adjoint role).
+template <typename R, int L, int NF, class H = BuiltinHam>
 cudaError_t launch_xpass(const PassArgs<R>& a, int rows, size_t smem, cudaStream_t st) {
     int kind = xkind_of(a.mode, a.epi);
     if (kind == XK_RK && a.want_obs && a.stage == 4) kind = XK_RKO;
     else if (kind == XK_RK && a.fuse_fwd) kind = XK_RKF;
     if (kind == XK_ADJ) {
-        if constexpr (NF == 1) return launch_xpass_kind<R, L, NF, XK_ADJ>(a, rows, smem, st);
+        if constexpr (NF == 1 && H::builtin) return launch_xpass_kind<R, L, NF, XK_ADJ, H>(a, rows, smem, st);
         return cudaErrorNotSupported;
     }
     switch (kind) {
-        case XK_FWD: return launch_xpass_kind<R, L, NF, XK_FWD>(a, rows, smem, st);
-        case XK_STORE: return launch_xpass_kind<R, L, NF, XK_STORE>(a, rows, smem, st);
-        case XK_RK: return launch_xpass_kind<R, L, NF, XK_RK>(a, rows, smem, st);
-        case XK_RKO: return launch_xpass_kind<R, L, NF, XK_RKO>(a, rows, smem, st);
-        case XK_RKF: return launch_xpass_kind<R, L, NF, XK_RKF>(a, rows, smem, st);
-        case XK_HB: return launch_xpass_kind<R, L, NF, XK_HB>(a, rows, smem, st);
-        case XK_RKI: return launch_xpass_kind<R, L, NF, XK_RKI>(a, rows, smem, st);
-        case XK_AH: return launch_xpass_kind<R, L, NF, XK_AH>(a, rows, smem, st);
-        default: return launch_xpass_kind<R, L, NF, XK_FULL>(a, rows, smem, st);
+        case XK_FWD: return launch_xpass_kind<R, L, NF, XK_FWD, H>(a, rows, smem, st);
+        case XK_STORE: return launch_xpass_kind<R, L, NF, XK_STORE, H>(a, rows, smem, st);
+        case XK_RK: return launch_xpass_kind<R, L, NF, XK_RK, H>(a, rows, smem, st);
+        case XK_RKO: return launch_xpass_kind<R, L, NF, XK_RKO, H>(a, rows, smem, st);
+        case XK_RKF: return launch_xpass_kind<R, L, NF, XK_RKF, H>(a, rows, smem, st);
+        case XK_HB: return launch_xpass_kind<R, L, NF, XK_HB, H>(a, rows, smem, st);
+        case XK_RKI: return launch_xpass_kind<R, L, NF, XK_RKI, H>(a, rows, smem, st);
+        case XK_AH: return launch_xpass_kind<R, L, NF, XK_AH, H>(a, rows, smem, st);
+        default: return launch_xpass_kind<R, L, NF, XK_FULL, H>(a, rows, smem, st);
     }
 }
 

@@ -99,7 +99,13 @@ typedef enum gpe_hamiltonian {
     GPE_HAM_BEC2 = 1,
     GPE_HAM_TEMPLATE = 2,
     GPE_HAM_DIPOLAR = 3,
-    GPE_HAM_SOFT = 4
+    GPE_HAM_SOFT = 4,
+    /* One component, the pointwise term supplied by a user plugin
+     * (gpe_set_user_hamiltonian, include/gpe_plugin.cuh): the counterpart of
+     * the reference's user-written Hamiltonian kernels
+     * (hamiltonians/BEC_oneComponent.hpp:8-22, the empty slot
+     * hamiltonians/single_template.cu:333-373). */
+    GPE_HAM_USER = 5
 } gpe_hamiltonian;
 
 /* Imaginary-time scheme.
@@ -289,6 +295,24 @@ gpe_status gpe_batch_imag_state(gpe_batch* b, int inst, double* out);
 /* Kernels of this library run for the batch so far (graph replays included). */
 long long  gpe_batch_kernel_launches(const gpe_batch* b);
 
+/* ---- user Hamiltonian plugins ------------------------------------------------
+ * A plugin is a shared library compiled from the user's .cu file with
+ * include/gpe_plugin.cuh: it instantiates this library's x-pass kernels with
+ * the user's pointwise functor (GPE_DEFINE_USER_HAMILTONIAN) and exports a
+ * function returning this table.  The launchers take the library's internal
+ * pass-argument block (opaque here), return 1 when they have a kernel for
+ * the line length L, and store the CUDA error code in *cuda_err. */
+typedef struct gpe_user_hamiltonian {
+    int abi_version; /* GPE_ABI_VERSION */
+    int (*launch_x_c64)(int L, const void* pass_args, int rows, size_t smem, void* stream, int* cuda_err);
+    int (*launch_x_c128)(int L, const void* pass_args, int rows, size_t smem, void* stream, int* cuda_err);
+} gpe_user_hamiltonian;
+/* Installs the plugin for a GPE_HAM_USER handle (the table must outlive the
+ * handle).  Every pass that evaluates the Hamiltonian then runs the plugin's
+ * kernels; a length the plugin was not built for fails with
+ * GPE_ERR_UNSUPPORTED.  The control gradient does not take user plugins. */
+gpe_status gpe_set_user_hamiltonian(gpe_handle* h, const gpe_user_hamiltonian* ops);
+
 /* ---- allocation-free norm (no counterpart in the reference) -------------
  * dev_out[0] = DV * sum |psi[i]|^2 over n complex128 points of a caller-owned
  * device array (interleaved re, im; 16-byte aligned), issued on cuda_stream
@@ -316,17 +340,22 @@ gpe_status gpe_norm_noalloc(const void* dev_psi_c128, long long n, double dv, do
  * (forward, forward*k-space*inverse, inverse) the implementation (scalar
  * lines, or two complex64 lines per thread with packed FP32x2 arithmetic),
  * the tile width, the resident CTAs per SM and the radix order of the line
- * FFT; per grid the x pass's rows per CTA.  Variant 0 / rows 0 are the
- * defaults, which every handle uses unless a tuning result applies.
+ * FFT; per grid the x pass's rows per CTA; for 3D complex64 grids with y and
+ * z lengths 64 or 128 (and nx a multiple of 4), whether the three strided
+ * passes of a stage run as one kernel over thread-block clusters (y-z slabs
+ * held in distributed shared memory, one read and one write of the work
+ * field).  Variant 0 / rows 0 / fused 0 are the defaults, which every handle
+ * uses unless a tuning result applies.
  *
  * gpe_tune times every variant that exists for cfg's grid (CUDA events on a
  * temporary handle: each strided pass alone, the rows by whole steps of the
  * workload, 0 = real-time RK4 steps, 1 = imaginary-time iterations), keeps
  * the fastest, and stores one line keyed by (nx, ny, nz, precision, fields,
  * instances = 1) in the JSON-lines file cache_path (replacing a line of the
- * same key; NULL = do not store).  report (may be NULL) receives 10 values:
+ * same key; NULL = do not store).  report (may be NULL) receives 11 values:
  * default and tuned microseconds per step, variants timed, the chosen
- * variants s[axis 1][mode 0..2], s[axis 2][mode 0..2], and the rows. */
+ * variants s[axis 1][mode 0..2], s[axis 2][mode 0..2], the rows and the
+ * fused y-z flag. */
 gpe_status gpe_tune(const gpe_config* cfg, int workload, const char* cache_path, double* report);
 /* Process-wide: gpe_create and gpe_batch_create apply the cache line that
  * matches a new handle (or batch group); NULL = read $GPE_TUNE_CACHE if set. */
@@ -337,10 +366,11 @@ gpe_status gpe_set_tune_cache(const char* path);
  * 2 values per group, default and tuned microseconds per iteration. */
 gpe_status gpe_batch_tune(gpe_batch* b, const char* cache_path, double* report);
 int        gpe_batch_groups(const gpe_batch* b);
-/* The handle's variants as 7 ints: s[1][0..2], s[2][0..2], rows.  Setting
- * checks that each variant exists (gpe_pass_variant_exists) for the grid. */
-gpe_status gpe_get_pass_variants(const gpe_handle* h, int* out7);
-gpe_status gpe_set_pass_variants(gpe_handle* h, const int* in7);
+/* The handle's variants as 8 ints: s[1][0..2], s[2][0..2], rows, fused y-z.
+ * Setting checks that each variant exists (gpe_pass_variant_exists) for the
+ * grid and that the fused kernel serves it. */
+gpe_status gpe_get_pass_variants(const gpe_handle* h, int* out8);
+gpe_status gpe_set_pass_variants(gpe_handle* h, const int* in8);
 /* 1 when strided-pass variant v (0 .. 11) exists for axis 1 (y) or 2 (z) of
  * cfg's grid, precision and fields; variant 0 always does.  Host only. */
 int        gpe_pass_variant_exists(const gpe_config* cfg, int axis, int v);
@@ -354,7 +384,8 @@ long long  gpe_kernel_launches(const gpe_handle* h);
  * unsynchronised host chrono, src/oneComponentGPSolver.cu:153,197-200) ----- */
 #define GPE_PROF_KINDS 6
 /* Pass kinds: 0 x-forward (+prologue), 1 x-inverse (+epilogue), 2 x-full,
- * 3 strided forward, 4 strided inverse, 5 strided forward*k-space*inverse. */
+ * 3 strided forward, 4 strided inverse, 5 strided forward*k-space*inverse
+ * (with the fused y-z kernel: that kernel, and no kinds 3 and 4). */
 /* When enabled, every pass launch is bracketed by CUDA events on the
  * handle's stream. */
 gpe_status gpe_profile_enable(gpe_handle* h, int enable);

@@ -109,9 +109,15 @@ def test_headline_apply_h_matches_oracle(gpu, prec, quench_start):
     g, o = pair(quench_cfg(prec), V, [psi0])
     gm, ge = g.apply_h(0.0, 0)
     om, oe = o.apply_h(0.0, 0)
-    tol = 1e-12 if prec == C128 else 2e-6
+    # complex64: the FP32 transforms of a 128^3 grid (21 radix stages forward
+    # and back) leave about 2e-6 of H psi.  The Laplacian alone of this smooth
+    # state is another matter: the transform's FP32 rounding (about 1e-7 of
+    # the spectrum, spread over all k) is weighted by k^2 up to the grid's
+    # cut-off while the Laplacian itself lives at small k, so its relative
+    # error is about 5e-5.
+    tol = 1e-12 if prec == C128 else 5e-6
     assert rel(gm, om) < tol and rel(ge, oe) < tol
-    assert rel(g.laplace(0), o.laplace(0)) < tol
+    assert rel(g.laplace(0), o.laplace(0)) < (1e-12 if prec == C128 else 2e-4)
     g.close()
 
 
