@@ -121,6 +121,8 @@ def lib() -> ctypes.CDLL:
         "gpe_set_tune_cache": (c_int, [ctypes.c_char_p]),
         "gpe_batch_tune": (c_int, [H, ctypes.c_char_p, P]),
         "gpe_batch_groups": (c_int, [H]),
+        "gpe_batch_set_persistent": (c_int, [H, c_int, ctypes.c_uint]),
+        "gpe_batch_persistent": (c_int, [H]),
         "gpe_get_pass_variants": (c_int, [H, POINTER(c_int)]),
         "gpe_set_pass_variants": (c_int, [H, POINTER(c_int)]),
         "gpe_pass_variant_exists": (c_int, [POINTER(GPEConfig), c_int, c_int]),
@@ -484,6 +486,16 @@ class Batch:
         rep = np.zeros(2 * max(ng, 1))
         _check(lib().gpe_batch_tune(self._h, cache_path.encode() if cache_path else None, _dp(rep)))
         return [(float(rep[2 * g]), float(rep[2 * g + 1])) for g in range(ng)]
+
+    def set_persistent(self, enable: bool = True, wait_bound: int = 0) -> None:
+        """One cooperative launch per RK4 stage for every instance
+        (gpe_batch_set_persistent); wait_bound: iterations a grid-barrier
+        wait may spin, 0 for the default (about a second)."""
+        _check(lib().gpe_batch_set_persistent(self._h, 1 if enable else 0, int(wait_bound)))
+
+    @property
+    def persistent(self) -> bool:
+        return bool(lib().gpe_batch_persistent(self._h))
 
     @property
     def launches(self) -> int:

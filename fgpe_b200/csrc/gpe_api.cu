@@ -182,7 +182,10 @@ __global__ void k_canon(C* A, C* B, const DevScalars* sc, int comp, int hb, long
 }
 __global__ void k_reset_iters(DevScalars* sc, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) sc[i].iters_done = 0;
+    if (i < n) {
+        sc[i].iters_done = 0;
+        sc[i].counter = 0;  // 0 after every complete launch; a launch cut short leaves it stale
+    }
 }
 __global__ void k_reset_scales(DevScalars* sc) {
     sc->scale[0][0] = sc->scale[0][1] = sc->scale[1][0] = sc->scale[1][1] = 1.0;
@@ -1740,6 +1743,14 @@ struct gpe_batch {
     bool use_graph = true;
     long long graph_launches = 0;        // kernels per replay of the graph
     long long replayed = 0;              // kernels run by graph replays
+    // persistent stage launches (gpe_batch_set_persistent): one cooperative
+    // launch per RK4 stage for every group
+    bool persistent = false;
+    unsigned wait_bound = 0;             // iterations a grid-barrier wait may spin
+    void* stage_args = nullptr;          // device PassArgs [4 stages][3 phases][BATCH_MAX_GROUPS]
+    GridBar* bar = nullptr;
+    int stage_grid = 0;                  // CTAs of the last stage launch
+    long long stage_launches = 0;        // stage kernels launched directly
 };
 
 namespace {
@@ -1766,8 +1777,117 @@ void batch_drop_graph(gpe_batch* b) {
     b->graph = nullptr;
 }
 
+// Bound of a grid-barrier wait when the caller gives none: 2^24 sleeps of
+// 64 ns or more (over a second), far beyond any phase of a stage.
+constexpr unsigned BATCH_WAIT_DEFAULT = 1u << 24;
+
+// Why the groups cannot run in the persistent stage kernel ("" when they can).
+std::string batch_persistent_reason(const gpe_batch* b) {
+    if (b->groups.size() > (size_t)BATCH_MAX_GROUPS) return "more than 8 grid geometries";
+    for (const gpe_handle* h : b->groups) {
+        if (h->cfg.imag_scheme != GPE_IMAG_RK4) return "imag_scheme is not GPE_IMAG_RK4";
+        if (h->nz != 1 || h->ny < 2) return "an instance grid is not two-dimensional (ny > 1, nz = 1)";
+        if (!batch_length_supported(h->nx) || !batch_length_supported(h->ny))
+            return "a grid length outside 64, 96, 128, 192, 256, 384, 512";
+        if (h->nf != 1 || h->ncomp != 1) return "an instance transforms more than one field";
+    }
+    return "";
+}
+
+// The pass arguments of every stage, phase and group, as imag_issue builds
+// them for run_chain (RK4 imaginary time; the batch's couplings are time
+// independent, so t = 0 as in the per-group iteration), uploaded once.
+template <typename R>
+gpe_status batch_build_stages(gpe_batch* b) {
+    typedef typename Cx<R>::T C;
+    const int ng = (int)b->groups.size();
+    std::vector<PassArgs<R>> host((size_t)4 * 3 * BATCH_MAX_GROUPS);
+    std::memset((void*)host.data(), 0, sizeof(PassArgs<R>) * host.size());
+    for (int s = 1; s <= 4; ++s) {
+        for (int g = 0; g < ng; ++g) {
+            gpe_handle* h = b->groups[g];
+            PassArgs<R> a = base_args<R>(h);
+            a.check_done = 1;
+            a.t = 0.0;
+            a.epi = EPI_RKI;
+            a.stage = s;
+            a.pro = (s == 1) ? PRO_A_SCALED : PRO_PIN;
+            for (int c = 0; c < 2; ++c) a.pin[c] = (const C*)h->B[c];
+            a.c_re = (s <= 2) ? -0.5 * h->cfg.dt : -1.0 * h->cfg.dt;
+            a.c_im = 0.0;
+            PassArgs<R>* ph = &host[(size_t)(s - 1) * 3 * BATCH_MAX_GROUPS + g];
+            // phase A: launch_x(XM_FWD)
+            ph[0] = a;
+            ph[0].mode = XM_FWD;
+            ph[0].tw = (const C*)h->tw[0];
+            // phase B: launch_s(axis 1, SM_FKI) with batch_rows(ny) x values per tile
+            PassArgs<R>& y = ph[BATCH_MAX_GROUPS];
+            y = a;
+            y.mode = SM_FKI;
+            y.sax = 1;
+            y.tx = batch_rows(h->ny);
+            y.tw = (const C*)h->tw[1];
+            y.tw2 = h->tw2[1];
+            y.sstride = h->nx;
+            y.ostride = (long long)h->nx * h->ny;
+            // phase C: launch_x(XM_INV), the EPI_RKI epilogue
+            ph[2 * BATCH_MAX_GROUPS] = a;
+            ph[2 * BATCH_MAX_GROUPS].mode = XM_INV;
+            ph[2 * BATCH_MAX_GROUPS].tw = (const C*)h->tw[0];
+        }
+    }
+    if (!b->stage_args) GPE_CUDA(cudaMalloc(&b->stage_args, sizeof(PassArgs<R>) * host.size()));
+    GPE_CUDA(cudaMemcpy(b->stage_args, host.data(), sizeof(PassArgs<R>) * host.size(), cudaMemcpyHostToDevice));
+    if (!b->bar) GPE_CUDA(cudaMalloc((void**)&b->bar, sizeof(GridBar)));
+    GPE_CUDA(cudaMemset(b->bar, 0, sizeof(GridBar)));
+    return GPE_OK;
+}
+
+// The tile lists of stage s: per group, its instances' x tiles (batch_rows(nx)
+// rows each) and strided tiles (batch_rows(ny) x values each), group-major.
+template <typename R>
+BatchStage<R> batch_stage_desc(const gpe_batch* b, int s, unsigned* max_tiles) {
+    BatchStage<R> d;
+    std::memset((void*)&d, 0, sizeof(d));
+    d.args = (const PassArgs<R>*)b->stage_args + (size_t)(s - 1) * 3 * BATCH_MAX_GROUPS;
+    d.ngroups = (int)b->groups.size();
+    unsigned xs = 0, ss = 0;
+    for (int g = 0; g < d.ngroups; ++g) {
+        const gpe_handle* h = b->groups[g];
+        const int rx = batch_rows(h->nx), ty = batch_rows(h->ny);
+        d.lx[g] = h->nx;
+        d.ly[g] = h->ny;
+        d.ntx[g] = (h->nx + ty - 1) / ty;
+        d.xt[g] = (unsigned)((h->ny * h->nz + rx - 1) / rx);
+        d.st[g] = (unsigned)(d.ntx[g] * h->nz);
+        d.xstart[g] = xs;
+        d.sstart[g] = ss;
+        xs += d.xt[g] * (unsigned)h->nb;
+        ss += d.st[g] * (unsigned)h->nb;
+    }
+    d.xstart[d.ngroups] = xs;
+    d.sstart[d.ngroups] = ss;
+    d.bar = b->bar;
+    d.wait_bound = b->wait_bound ? b->wait_bound : BATCH_WAIT_DEFAULT;
+    *max_tiles = std::max(xs, ss);
+    return d;
+}
+
+template <typename R>
+gpe_status batch_issue_stages(gpe_batch* b) {
+    for (int s = 1; s <= 4; ++s) {
+        unsigned max_tiles = 0;
+        const BatchStage<R> d = batch_stage_desc<R>(b, s, &max_tiles);
+        const cudaError_t e = launch_batch_stage(d, max_tiles, b->st, &b->stage_grid);
+        if (e != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("batch stage launch: ") + cudaGetErrorString(e));
+        b->stage_launches++;
+    }
+    return GPE_OK;
+}
+
 template <typename R>
 gpe_status batch_issue_iteration(gpe_batch* b) {
+    if (b->persistent) return batch_issue_stages<R>(b);
     for (gpe_handle* h : b->groups) GPE_TRY(imag_issue<R>(h, 0, 1));
     return GPE_OK;
 }
@@ -1780,10 +1900,11 @@ gpe_status batch_capture(gpe_batch* b) {
         b->use_graph = false;  // the legacy default stream cannot be captured
         return GPE_OK;
     }
-    long long before = 0, after = 0;
+    long long before = b->stage_launches, after = 0;
     for (gpe_handle* h : b->groups) before += h->launches;
     GPE_CUDA(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
     gpe_status s = batch_issue_iteration<R>(b);
+    after = b->stage_launches;
     for (gpe_handle* h : b->groups) after += h->launches;
     // captured launches have not run: count them per replay instead
     b->graph_launches = after - before;
@@ -1813,6 +1934,7 @@ gpe_status batch_capture(gpe_batch* b) {
 template <typename R>
 gpe_status batch_step_imag_t(gpe_batch* b, int nsteps, int* iters_done, int* converged) {
     for (gpe_handle* h : b->groups) GPE_TRY(imag_prepare<R>(h));
+    if (b->persistent) GPE_CUDA(cudaMemsetAsync(b->bar, 0, sizeof(GridBar), b->st));
     GPE_TRY(batch_capture<R>(b));
     for (int j = 0; j < nsteps; ++j) {
         if (b->exec) {
@@ -1824,6 +1946,12 @@ gpe_status batch_step_imag_t(gpe_batch* b, int nsteps, int* iters_done, int* con
     }
     GPE_CUDA(cudaStreamSynchronize(b->st));
     GPE_CUDA(cudaGetLastError());
+    if (b->persistent) {
+        GridBar bar;
+        GPE_CUDA(cudaMemcpy(&bar, b->bar, sizeof(bar), cudaMemcpyDeviceToHost));
+        if (bar.status == GPE_ERR_TIMEOUT)
+            return fail(GPE_ERR_TIMEOUT, "a grid-barrier wait of the persistent batch kernel expired");
+    }
     bool diverged = false;
     std::vector<DevScalars> sv;
     for (size_t g = 0; g < b->groups.size(); ++g) {
@@ -1908,6 +2036,8 @@ gpe_status gpe_batch_destroy(gpe_batch* b) {
     if (!b) return GPE_OK;
     cudaStreamSynchronize(b->st);
     batch_drop_graph(b);
+    if (b->stage_args) cudaFree(b->stage_args);
+    if (b->bar) cudaFree(b->bar);
     for (gpe_handle* h : b->groups) {
         free_all(h);
         delete h;
@@ -1978,9 +2108,26 @@ gpe_status gpe_batch_imag_state(gpe_batch* b, int inst, double* out) {
     return GPE_OK;
 }
 
+gpe_status gpe_batch_set_persistent(gpe_batch* b, int enable, unsigned int wait_bound) {
+    if (!b) return fail(GPE_ERR_INVALID_ARG, "null batch");
+    if (enable) {
+        const std::string why = batch_persistent_reason(b);
+        if (!why.empty()) return fail(GPE_ERR_UNSUPPORTED, "persistent batch launch: " + why);
+        GPE_CUDA(cudaStreamSynchronize(b->st));
+        GPE_TRY(b->prec == GPE_C64 ? batch_build_stages<float>(b) : batch_build_stages<double>(b));
+    }
+    batch_drop_graph(b);  // the captured launches carry the old choice and bound
+    b->persistent = enable != 0;
+    b->wait_bound = wait_bound;
+    b->use_graph = true;
+    return GPE_OK;
+}
+
+int gpe_batch_persistent(const gpe_batch* b) { return (b && b->persistent) ? 1 : 0; }
+
 long long gpe_batch_kernel_launches(const gpe_batch* b) {
     if (!b) return 0;
-    long long n = b->replayed;
+    long long n = b->replayed + b->stage_launches;
     for (const gpe_handle* h : b->groups) n += h->launches;
     return n;
 }

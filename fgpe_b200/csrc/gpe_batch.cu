@@ -1,0 +1,69 @@
+// gpe_batch.cu -- launcher of the persistent batch stage kernel (gpe_batch.cuh).
+#include <atomic>
+
+#include "gpe_batch.cuh"
+
+namespace gpe {
+
+// Dynamic shared memory of the stage kernel: the largest tile of the lengths
+// it serves.
+size_t batch_stage_smem(int esz) {
+    size_t m = 0;
+#define GPE_BATCH_SM(L) m = m > batch_smem(L, esz) ? m : batch_smem(L, esz);
+    GPE_BATCH_LENGTHS(GPE_BATCH_SM)
+#undef GPE_BATCH_SM
+    return m;
+}
+
+bool batch_length_supported(int L) { return batch_length_ok(L); }
+
+template <typename R>
+static cudaError_t launch_stage(const BatchStage<R>& b, unsigned max_tiles, cudaStream_t st, int* grid_out) {
+    const size_t smem = batch_stage_smem((int)sizeof(typename Cx<R>::T));
+    static std::atomic<unsigned long long> attr{0};
+    cudaError_t e = allow_smem(k_batch_stage<R>, smem, attr);
+    if (e != cudaSuccess) return e;
+    // CTAs per SM and SMs of each device, looked up once
+    constexpr int MAXDEV = 64;
+    static std::atomic<int> cached[MAXDEV];
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    int per_sm = 0, nsm = 0;
+    const int c = (dev >= 0 && dev < MAXDEV) ? cached[dev].load() : 0;
+    if (c > 0) {
+        per_sm = c & 0xffff;
+        nsm = c >> 16;
+    } else {
+        if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_stage<R>, BATCH_THREADS, smem)) !=
+            cudaSuccess)
+            return e;
+        if (dev >= 0 && dev < MAXDEV && per_sm > 0 && per_sm < 0x10000 && nsm < 0x8000)
+            cached[dev].store(per_sm | (nsm << 16));
+    }
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    // co-resident CTAs (the cooperative launch checks it), no more than the tiles
+    unsigned grid = (unsigned)(per_sm * nsm);
+    if (max_tiles < grid) grid = max_tiles > 0 ? max_tiles : 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(BATCH_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    if (grid_out) *grid_out = (int)grid;
+    return cudaLaunchKernelEx(&cfg, k_batch_stage<R>, b);
+}
+
+cudaError_t launch_batch_stage(const BatchStage<float>& b, unsigned max_tiles, cudaStream_t st, int* grid) {
+    return launch_stage<float>(b, max_tiles, st, grid);
+}
+cudaError_t launch_batch_stage(const BatchStage<double>& b, unsigned max_tiles, cudaStream_t st, int* grid) {
+    return launch_stage<double>(b, max_tiles, st, grid);
+}
+
+}  // namespace gpe

@@ -3,6 +3,7 @@
 // precision, gpe_inst_*.cu).
 #pragma once
 
+#include "gpe_batch_args.cuh"
 #include "gpe_kernels.cuh"
 
 namespace gpe {

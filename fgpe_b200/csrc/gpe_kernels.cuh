@@ -201,13 +201,32 @@ __host__ __device__ constexpr SVar svar(int esz, int L, int v) {
 }
 
 // ---- shared-memory line addressing -----------------------------------------
-// X pass exchange rows are padded by one slot every 8 elements: the first
-// radix-8 Stockham pass stores with stride 8, which would put the 16 lanes of
-// a row on two bank pairs without the padding.
-__host__ __device__ constexpr int xpad(int L) { return L + (L >> 3); }
-template <typename C> struct RowAddr {      // X pass: S[b*xpad(L) + pos + pos/8]
+// X pass exchange rows: line position pos of row b at S[b*xpad(L) + xmap(L, pos)].
+// A half warp (16 lanes of 8-byte values) is one 128-byte wavefront when its
+// lanes fall on distinct bank pairs.  The Stockham exchanges of a row store
+// and load with strides 1, 2, 8, 16 ... (the radix-8 stores of the forward
+// plan, the radix-2 stores that start the reversed inverse plan), so the map
+// is chosen per length by counting the wavefronts of every exchange of both
+// plans: an XOR of the low four bits with a higher bit field for the long
+// powers of two and for 192/384 (no padding), a double padding for 64 and
+// 96, one slot every 8 otherwise.  The map only places values; the
+// arithmetic and its results do not depend on it.
+__host__ __device__ constexpr int xmap(int L, int pos) {
+    return (L == 128 || L == 256 || L == 512 || L == 1024) ? (pos ^ ((pos >> 3) & 15))
+           : (L == 192 || L == 384)                       ? (pos ^ ((pos >> 2) & 15))
+           : (L == 64)                                    ? (pos + (pos >> 3) + (pos >> 5))
+           : (L == 96)                                    ? (pos + 2 * (pos >> 3) + (pos >> 5))
+                                                          : (pos + (pos >> 3));
+}
+// Row stride: one past the largest mapped position.
+__host__ __device__ constexpr int xpad(int L) {
+    return (L == 128 || L == 256 || L == 512 || L == 1024 || L == 192 || L == 384) ? L
+           : (L == 64 || L == 96)                                                 ? xmap(L, L - 1) + 1
+                                                                                  : L + (L >> 3);
+}
+template <typename C, int L> struct RowAddr {  // X pass: S[b*xpad(L) + xmap(L, pos)]
     C* base;
-    __device__ __forceinline__ C* operator()(unsigned pos) const { return base + (pos + (pos >> 3)); }
+    __device__ __forceinline__ C* operator()(unsigned pos) const { return base + xmap(L, (int)pos); }
 };
 template <typename C, int TX> struct ColAddr {  // strided pass: S[pos*TX + b]
     C* base;

@@ -38,16 +38,19 @@ struct InstPtr {
 };
 
 template <typename R>
-__device__ __forceinline__ InstPtr select_instance(const PassArgs<R>& a) {
+__device__ __forceinline__ InstPtr select_instance_at(const PassArgs<R>& a, unsigned inst) {
     InstPtr p{a.sc, a.prms, a.partials, 0};
     if (a.nbatch > 1) {
-        const int inst = blockIdx.y;
         p.sc += inst;
         p.prms += (size_t)inst * GPE_NO_HAMIL_PARAMS;
         p.partials += (size_t)inst * a.pstride;
         p.boff = (long long)inst * a.bstride;
     }
     return p;
+}
+template <typename R>
+__device__ __forceinline__ InstPtr select_instance(const PassArgs<R>& a) {
+    return select_instance_at(a, a.nbatch > 1 ? blockIdx.y : 0u);
 }
 
 // Lazy normalisation factors of the current / previous heavy-ball slot.
@@ -236,12 +239,15 @@ __device__ void finalize_scalars(const PassArgs<R>& a, DevScalars* sc, const dou
     }
 }
 
+// bidx: this tile's partial slot; nblk: the tiles of the instance (the last
+// of them to arrive finalises).
 template <typename R, int NQ>
-__device__ void reduce_and_finalize(const PassArgs<R>& a, const InstPtr& ip, DD (&acc)[NQ], DD* red) {
+__device__ void reduce_and_finalize(const PassArgs<R>& a, const InstPtr& ip, DD (&acc)[NQ], DD* red, unsigned bidx,
+                                    unsigned nblk) {
     __shared__ int is_last;
     block_reduce<NQ>(acc, red);
     if (threadIdx.x == 0) {
-        double* p = ip.partials + (size_t)blockIdx.x * NQ * 2;
+        double* p = ip.partials + (size_t)bidx * NQ * 2;
 #pragma unroll
         for (int q = 0; q < NQ; ++q) {
             p[2 * q] = acc[q].s;
@@ -249,7 +255,7 @@ __device__ void reduce_and_finalize(const PassArgs<R>& a, const InstPtr& ip, DD 
         }
         __threadfence();
         const unsigned int ticket = atomicAdd(&ip.sc->counter, 1u);
-        is_last = (ticket == gridDim.x - 1) ? 1 : 0;
+        is_last = (ticket == nblk - 1) ? 1 : 0;
     }
     __syncthreads();
     if (is_last) {
@@ -257,7 +263,7 @@ __device__ void reduce_and_finalize(const PassArgs<R>& a, const InstPtr& ip, DD 
         DD s[NQ];
 #pragma unroll
         for (int q = 0; q < NQ; ++q) s[q] = DD{0.0, 0.0};
-        const unsigned int nb = gridDim.x;
+        const unsigned int nb = nblk;
         for (unsigned int i = threadIdx.x; i < nb; i += blockDim.x) {
             const double* p = ip.partials + (size_t)i * NQ * 2;
 #pragma unroll
@@ -722,34 +728,28 @@ __device__ __forceinline__ void prefetch_rk_inputs(const PassArgs<R>& a, long lo
     }
 }
 
+// One tile of an x pass: `rows` rows from row tile*rows of instance inst
+// (ntiles tiles per instance), after the kernel's wait on the previous grid.
+// k_xpass runs one tile per CTA; the persistent batch kernel loops over tiles.
 template <typename R, int L, int NF, int KIND, class H = BuiltinHam>
-__global__ void __launch_bounds__(256, (xpass_min_blocks<R, L, NF, KIND>())) k_xpass(PassArgs<R> a, int rows) {
+__device__ __forceinline__ void xpass_tile(const PassArgs<R>& a, int rows, unsigned tile, unsigned inst,
+                                           unsigned ntiles, unsigned char* smem_raw) {
     typedef typename Cx<R>::T C;
     constexpr int E = Plan<L>::E;
     constexpr int T = Plan<L>::T;
     constexpr int RinF = Plan<L>::in_radix(false);
     constexpr int RoutF = Plan<L>::out_radix(false);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const InstPtr ip = select_instance(a);
+    const InstPtr ip = select_instance_at(a, inst);
     const long long boff = ip.boff;
-    if constexpr (KIND == XK_RKF || KIND == XK_RK || KIND == XK_RKO) {
-        // The epilogue inputs were written two or more launches earlier, so
-        // the L2 prefetch may run before the wait for the preceding grid
-        // (with programmatic launch this CTA can start during its tail);
-        // a prefetch is only a cache hint either way.
-        const int nr = min(rows, a.nrows - (int)blockIdx.x * rows);
-        if (nr > 0) prefetch_rk_inputs<R, NF>(a, boff + (long long)blockIdx.x * rows * L, nr, L);
-    }
-    pass_prologue_sync();
     if (a.check_done && ip.sc->done) return;
 
     C* X = reinterpret_cast<C*>(smem_raw);
     const unsigned b = threadIdx.x / T, t = threadIdx.x % T;
-    const int row = blockIdx.x * rows + (int)b;
+    const int row = (int)tile * rows + (int)b;
     const bool valid = row < a.nrows;
     // g0 + reg_off(e): global index of register e of this thread's line
     const long long g0 = boff + (long long)(valid ? row : 0) * L + t;
-    const RowAddr<C> addr{X + b * xpad(L)};
+    const RowAddr<C, L> addr{X + b * xpad(L)};
     const int cur = ip.sc->cur_slot;
     const PsiScale<R> ps = load_scales<R>(ip.sc, cur);
     DD acc[MAXQ];
@@ -828,10 +828,26 @@ __global__ void __launch_bounds__(256, (xpass_min_blocks<R, L, NF, KIND>())) k_x
         if constexpr (kind_reduces<KIND>()) {
             if (epi_reduces(a)) {
                 __shared__ DD red[32 * MAXQ];
-                reduce_and_finalize<R, MAXQ>(a, ip, acc, red);
+                reduce_and_finalize<R, MAXQ>(a, ip, acc, red, tile, ntiles);
             }
         }
     }
+}
+
+template <typename R, int L, int NF, int KIND, class H = BuiltinHam>
+__global__ void __launch_bounds__(256, (xpass_min_blocks<R, L, NF, KIND>())) k_xpass(PassArgs<R> a, int rows) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    if constexpr (KIND == XK_RKF || KIND == XK_RK || KIND == XK_RKO) {
+        // The epilogue inputs were written two or more launches earlier, so
+        // the L2 prefetch may run before the wait for the preceding grid
+        // (with programmatic launch this CTA can start during its tail);
+        // a prefetch is only a cache hint either way.
+        const long long boff = select_instance(a).boff;
+        const int nr = min(rows, a.nrows - (int)blockIdx.x * rows);
+        if (nr > 0) prefetch_rk_inputs<R, NF>(a, boff + (long long)blockIdx.x * rows * L, nr, L);
+    }
+    pass_prologue_sync();
+    xpass_tile<R, L, NF, KIND, H>(a, rows, blockIdx.x, a.nbatch > 1 ? blockIdx.y : 0u, gridDim.x, smem_raw);
 }
 
 // ---- strided pass -----------------------------------------------------------------
@@ -850,21 +866,24 @@ __host__ __device__ constexpr int spass_min_blocks() {
 // TX: x values per CTA (tile width); MB: resident CTAs per SM the launch
 // bounds ask for.  The defaults are spass_tx and spass_min_blocks; other
 // (TX, MB) pairs are autotuner variants (gpe_tune.cu).
-template <typename R, int L, int NF, int TX, int MB>
-__global__ void __launch_bounds__(TX * Plan<L>::T, MB) k_spass(PassArgs<R> a, int ntx) {
+// One tile of a strided pass (tile = outer * ntx + x block) of instance inst,
+// after the kernel's wait on the previous grid; k_spass runs one tile per
+// CTA, the persistent batch kernel loops over tiles.
+template <typename R, int L, int NF, int TX>
+__device__ __forceinline__ void spass_tile(const PassArgs<R>& a, int ntx, unsigned tile, unsigned inst,
+                                           unsigned char* smem_raw) {
     typedef typename Cx<R>::T C;
     constexpr int E = Plan<L>::E;
     constexpr int T = Plan<L>::T;
     constexpr int RinF = Plan<L>::in_radix(false);
     constexpr int RoutF = Plan<L>::out_radix(false);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    pass_prologue_sync();
-    const long long boff = select_instance(a).boff;
-    if (a.check_done && (a.sc + (a.nbatch > 1 ? blockIdx.y : 0))->done) return;
+    const InstPtr ip = select_instance_at(a, inst);
+    const long long boff = ip.boff;
+    if (a.check_done && ip.sc->done) return;
 
     C* X = reinterpret_cast<C*>(smem_raw);
     constexpr int tx = TX;
-    const int xb = blockIdx.x % ntx, outer = blockIdx.x / ntx;
+    const int xb = (int)tile % ntx, outer = (int)tile / ntx;
     const int x0 = xb * tx;
     const unsigned b = threadIdx.x % tx, t = threadIdx.x / tx;
     const bool valid = x0 + (int)b < a.nx;
@@ -932,6 +951,13 @@ __global__ void __launch_bounds__(TX * Plan<L>::T, MB) k_spass(PassArgs<R> a, in
             for (int f = 0; f < NF; ++f) a.w[f][gi] = v[f][e];
         }
     }
+}
+
+template <typename R, int L, int NF, int TX, int MB>
+__global__ void __launch_bounds__(TX * Plan<L>::T, MB) k_spass(PassArgs<R> a, int ntx) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    pass_prologue_sync();
+    spass_tile<R, L, NF, TX>(a, ntx, blockIdx.x, a.nbatch > 1 ? blockIdx.y : 0u, smem_raw);
 }
 
 // ---- paired complex64 strided pass ------------------------------------------------

@@ -3,7 +3,8 @@
 // (h_mu = T + (V + 4 pi a(t) |psi|^2) psi, h_en with 2 pi a(t), a(t) the
 // quench profile d_quench_as of prms[0..5]) as a user functor.  It is the
 // example for plugin authors and the test of the plug-point: a handle with
-// GPE_HAM_USER and this plugin must reproduce GPE_HAM_BEC bit for bit.
+// GPE_HAM_USER and this plugin must reproduce GPE_HAM_BEC to the rounding of
+// the precision.
 #define GPE_USER_SIZES(X) X(16) X(32) X(64) X(128)
 #include "gpe_plugin.cuh"
 

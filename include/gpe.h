@@ -294,6 +294,19 @@ gpe_status gpe_batch_step_imag(gpe_batch* b, int nsteps, int* iters_done, int* c
 gpe_status gpe_batch_imag_state(gpe_batch* b, int inst, double* out);
 /* Kernels of this library run for the batch so far (graph replays included). */
 long long  gpe_batch_kernel_launches(const gpe_batch* b);
+/* Persistent launches: one cooperative kernel per RK4 stage runs the stage's
+ * three passes for every instance of every group, with a grid-wide barrier
+ * between the passes (4 launches an iteration instead of 12 per group).
+ * Needs GPE_IMAG_RK4, two-dimensional grids (ny > 1, nz = 1) of lengths 64,
+ * 96, 128, 192, 256, 384 or 512, and at most 8 geometry groups; else
+ * GPE_ERR_UNSUPPORTED.  wait_bound: iterations a barrier wait may spin
+ * (0 = about a second); a wait that runs out ends the launch and
+ * gpe_batch_step_imag returns GPE_ERR_TIMEOUT (the state of that call is
+ * then undefined; the next call starts clean).  enable = 0 restores the
+ * per-group launches.  No counterpart in the reference (one instance per
+ * process). */
+gpe_status gpe_batch_set_persistent(gpe_batch* b, int enable, unsigned int wait_bound);
+int        gpe_batch_persistent(const gpe_batch* b);
 
 /* ---- user Hamiltonian plugins ------------------------------------------------
  * A plugin is a shared library compiled from the user's .cu file with

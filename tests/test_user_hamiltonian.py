@@ -2,7 +2,8 @@
 the example plugin fgpe_b200/plugins/user_bec.cu re-implements the
 one-component BEC term (hamiltonians/BEC_oneComponent.cu:128-178) as a user
 functor compiled in its own library; a GPE_HAM_USER handle with it must
-reproduce the built-in GPE_HAM_BEC handle bit for bit."""
+reproduce the built-in GPE_HAM_BEC handle to the rounding of the precision
+(1e-13 relative in complex128, 1e-6 in complex64)."""
 import ctypes
 import os
 
@@ -63,9 +64,14 @@ def test_user_plugin_reproduces_builtin_bec(gpu, prec, shape):
                 s.set_psi(0, psi)
                 r += [s.step_real(0, 5, want_obs=True), s.get_psi(0)]
                 out[(ham, scheme)] = r
+    # The plugin runs the same arithmetic, compiled in another translation
+    # unit: the compiler may fuse a multiply-add differently there, so the
+    # results agree to the last bits of the precision, not bit for bit.
+    tol = 1e-13 if prec == C128 else 1e-6
     for scheme in (0, IMAG_RK4):
         for a, b in zip(out[(HAM_BEC, scheme)], out[(HAM_USER, scheme)]):
-            assert np.array_equal(np.asarray(a), np.asarray(b))
+            a, b = np.asarray(a).ravel(), np.asarray(b).ravel()
+            assert np.linalg.norm(a - b) <= tol * np.linalg.norm(a)
 
 
 @pytest.mark.gpu
