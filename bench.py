@@ -590,19 +590,37 @@ def run_sweep(args):
     # autotune every geometry group in place: per group the default and the
     # tuned microseconds per iteration, measured on the same work
     tune_rep = None if args.no_tune else b.tune(os.path.join("/tmp", f"gpe_tune_{os.getpid()}.jsonl"))
-    for i, (c, V, p, *_ ) in enumerate(inst):
-        b.set_vext(i, V)
-        b.set_psi(i, p)
-    b.step_imag(W)
-    torch.cuda.synchronize()
-    l0 = b.launches
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    it, cv = b.step_imag(K)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    launches = b.launches - l0
+    def timed(persistent):
+        """W warm-up and K timed iterations of every instance from the seeded
+        start, under per-group or persistent stage launches."""
+        b.set_persistent(persistent)
+        for i, (c, V, p, *_ ) in enumerate(inst):
+            b.set_vext(i, V)
+            b.set_psi(i, p)
+        b.step_imag(W)
+        torch.cuda.synchronize()
+        l0 = b.launches
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        it, cv = b.step_imag(K)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), it, cv, b.launches - l0
+
+    # both launch modes on the same work; the faster one is the headline
+    modes = {"per_group": timed(False)}
+    try:
+        modes["persistent"] = timed(True)
+    except gp.GPEError as e:
+        modes["persistent"] = str(e)
+    best = min((k for k in modes if not isinstance(modes[k], str)), key=lambda k: modes[k][0])
+    b.set_persistent(best == "persistent")
+    ms, it, cv, launches = modes[best]
+    launch_modes = {k: (v if isinstance(v, str) else
+                        {"ms_per_step": round(v[0] / K, 4), "launches_per_iteration": round(v[3] / K, 2),
+                         "instance_steps_per_s": round(int(v[1].sum()) / (v[0] / 1e3), 1)})
+                    for k, v in modes.items()}
+    launch_modes["chosen"] = best
     inst_steps = int(it.sum())
     if dist is not None:
         t = torch.tensor([ms, float(inst_steps)], dtype=torch.float64, device="cuda")
@@ -667,7 +685,7 @@ def run_sweep(args):
                          "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": round(alg_bytes / (ms / 1e3) / 1e9 / peak, 4), "traffic": None,
                          "model": "45 F per RK4 imaginary iteration, F = N*8 B"},
-            "tuning": tuning_summary(tune_rep, inst),
+            "tuning": tuning_summary(tune_rep, inst), "launch_modes": launch_modes,
             "gpu_launches": launches, "convergence": conv,
             "cpu_baseline": sweep_cpu_leg(everything, stream)}
     if world > 1:
@@ -823,9 +841,11 @@ def run_control(args):
     # central stencil (-L(u+2h) + 8 L(u+h) - 8 L(u-h) + L(u-2h)) / 12h, whose
     # truncation error (h^4) stays far below the 1e-4 bar; the second-order
     # stencil's h^2 L''' term alone reaches ~5e-5 on this nearly degenerate
-    # loss (L ~ 1 - 3e-7)
+    # loss (L ~ 1 - 3e-7).  h = 1e-3: at 1e-4 the loss's own rounding (its
+    # FP64 reductions over 65536 points, ~1e-13 of L) divided by h already
+    # reaches ~1e-4 of the small gradient components
     rng = np.random.default_rng(7)
-    h = 1e-4
+    h = 1e-3
     s128 = solvers["c128"]
     L128, g128 = s128.control_gradient(u, target, 50)
     errs = []

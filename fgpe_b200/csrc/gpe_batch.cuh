@@ -36,6 +36,13 @@ __device__ __forceinline__ unsigned ld_volatile_u(const unsigned* p) {
 }
 __device__ __forceinline__ int ld_volatile_i(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
 
+// Every tile uses all the threads: rows x T = 256 for the x tiles, x values x
+// T for the strided ones (T = the line's threads), so no thread of a CTA
+// indexes past its tile.
+#define GPE_BATCH_FULL(L) static_assert(batch_rows(L) * (L / make_plan(L).E) == BATCH_THREADS, "tile of " #L);
+GPE_BATCH_LENGTHS(GPE_BATCH_FULL)
+#undef GPE_BATCH_FULL
+
 // Grid-wide barrier with a bounded wait; false when any CTA gave up (then the
 // caller leaves the kernel).
 __device__ __forceinline__ bool grid_sync_bounded(GridBar* bar, unsigned bound) {
