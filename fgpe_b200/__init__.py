@@ -123,6 +123,7 @@ def lib() -> ctypes.CDLL:
         "gpe_batch_groups": (c_int, [H]),
         "gpe_batch_set_persistent": (c_int, [H, c_int, ctypes.c_uint]),
         "gpe_batch_persistent": (c_int, [H]),
+        "gpe_batch_persistent_info": (c_int, [H, POINTER(c_longlong)]),
         "gpe_get_pass_variants": (c_int, [H, POINTER(c_int)]),
         "gpe_set_pass_variants": (c_int, [H, POINTER(c_int)]),
         "gpe_pass_variant_exists": (c_int, [POINTER(GPEConfig), c_int, c_int]),
@@ -496,6 +497,14 @@ class Batch:
     @property
     def persistent(self) -> bool:
         return bool(lib().gpe_batch_persistent(self._h))
+
+    def persistent_info(self) -> dict:
+        """Resources of the persistent stage kernel (gpe_batch_persistent_info)."""
+        out = (c_longlong * 9)()
+        _check(lib().gpe_batch_persistent_info(self._h, out))
+        keys = ("registers", "static_smem", "max_threads", "local_bytes", "ctas_per_sm", "sms", "cooperative",
+                "dynamic_smem", "last_grid")
+        return dict(zip(keys, (int(v) for v in out)))
 
     @property
     def launches(self) -> int:

@@ -1084,7 +1084,7 @@ gpe_status ctrl_stage_args(gpe_handle* h, void* S, void* Pa, void* Pb, void* Pc,
         a.t = (s == 1) ? (double)n * dt : (n + 0.5) * dt;
         a.want_obs = 0;
         a.fuse_fwd = (can_fuse && s < 3) ? 1 : 0;
-        GPE_TRY(run_chain<R>(h, a, 1, w_ready));
+        GPE_TRY(run_chain<R>(h, a, h->nf, w_ready));
         w_ready = a.fuse_fwd != 0;
     }
     h->w_fwd_A = false;
@@ -1118,7 +1118,7 @@ gpe_status ctrl_adjoint_step(gpe_handle* h, void* S, void* Pa, void* Pb, void* P
         a.c_re = cl[s];
         a.c_im = cj[s];
         a.t = (s == 1) ? (double)n * dt : (s < 4) ? (n + 0.5) * dt : (double)(n + 1) * dt;
-        GPE_TRY(run_chain<R>(h, a, 1));
+        GPE_TRY(run_chain<R>(h, a, h->nf));
     }
     h->w_fwd_A = false;
     GPE_CUDA(cudaGetLastError());
@@ -1697,9 +1697,12 @@ gpe_status gpe_profile_read(gpe_handle* h, double* ms_out, long long* count_out)
 
 gpe_status gpe_control_set_basis(gpe_handle* h, int nctrl, const double* host_G) {
     GPE_TRY(check_handle(h));
-    if (h->ncomp != 1 || h->cfg.hamiltonian != GPE_HAM_BEC || h->nb != 1 || h->cfg.prms[11] != 0)
+    const int ham = h->cfg.hamiltonian;
+    if (h->ncomp != 1 || (ham != GPE_HAM_BEC && ham != GPE_HAM_DIPOLAR && ham != GPE_HAM_SOFT) || h->nb != 1 ||
+        h->cfg.prms[11] != 0)
         return fail(GPE_ERR_UNSUPPORTED,
-                    "the control gradient needs one component, GPE_HAM_BEC and no moving-frame term");
+                    "the control gradient needs one component, GPE_HAM_BEC, GPE_HAM_DIPOLAR or GPE_HAM_SOFT, "
+                    "and no moving-frame term");
     if (nctrl < 1 || nctrl > 64 || !host_G) return fail(GPE_ERR_INVALID_ARG, "nctrl must be 1..64 with a basis");
     const size_t rs = h->prec == GPE_C64 ? 4 : 8;
     if (h->ctrlG) cudaFree(h->ctrlG);
@@ -1751,6 +1754,10 @@ struct gpe_batch {
     GridBar* bar = nullptr;
     int stage_grid = 0;                  // CTAs of the last stage launch
     long long stage_launches = 0;        // stage kernels launched directly
+    // early stop: per chunk of iterations, whether any instance still runs
+    int* d_running = nullptr;            // device [2], one per chunk slot
+    int* flag_host = nullptr;            // pinned [2]
+    cudaEvent_t flag_ev[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -1878,8 +1885,14 @@ gpe_status batch_issue_stages(gpe_batch* b) {
     for (int s = 1; s <= 4; ++s) {
         unsigned max_tiles = 0;
         const BatchStage<R> d = batch_stage_desc<R>(b, s, &max_tiles);
-        const cudaError_t e = launch_batch_stage(d, max_tiles, b->st, &b->stage_grid);
-        if (e != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("batch stage launch: ") + cudaGetErrorString(e));
+        BatchLaunchInfo li{0, 0, 0, 0};
+        const cudaError_t e = launch_batch_stage(d, max_tiles, b->st, &li);
+        b->stage_grid = li.grid;
+        if (e != cudaSuccess)
+            return fail(GPE_ERR_CUDA, std::string("batch stage launch: ") + cudaGetErrorString(e) + " (CTAs per SM " +
+                                          std::to_string(li.per_sm) + ", SMs " + std::to_string(li.nsm) + ", grid " +
+                                          std::to_string(li.grid) + ", dynamic shared memory " +
+                                          std::to_string(li.smem) + " B)");
         b->stage_launches++;
     }
     return GPE_OK;
@@ -1931,18 +1944,56 @@ gpe_status batch_capture(gpe_batch* b) {
     return GPE_OK;
 }
 
+// Sets *running when any of the n instances has not converged (or failed).
+__global__ void k_any_running(const DevScalars* sc, int n, int* running) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (!sc[i].done) *running = 1;
+}
+
+gpe_status batch_flags(gpe_batch* b) {
+    if (b->flag_host) return GPE_OK;
+    GPE_CUDA(cudaMalloc((void**)&b->d_running, 2 * sizeof(int)));
+    GPE_CUDA(cudaHostAlloc((void**)&b->flag_host, 2 * sizeof(int), cudaHostAllocDefault));
+    for (cudaEvent_t& ev : b->flag_ev) GPE_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    return GPE_OK;
+}
+
+// Iterations are issued in chunks of IMAG_CHUNK as for one handle: after
+// each chunk a flag (any instance still running) lands in pinned memory, the
+// host reads the previous chunk's flag while the next chunk is queued, and
+// stops issuing once every instance has converged.
 template <typename R>
 gpe_status batch_step_imag_t(gpe_batch* b, int nsteps, int* iters_done, int* converged) {
     for (gpe_handle* h : b->groups) GPE_TRY(imag_prepare<R>(h));
     if (b->persistent) GPE_CUDA(cudaMemsetAsync(b->bar, 0, sizeof(GridBar), b->st));
     GPE_TRY(batch_capture<R>(b));
-    for (int j = 0; j < nsteps; ++j) {
-        if (b->exec) {
-            GPE_CUDA(cudaGraphLaunch(b->exec, b->st));
-            b->replayed += b->graph_launches;
-        } else {
-            GPE_TRY(batch_issue_iteration<R>(b));
+    GPE_TRY(batch_flags(b));
+    int issued = 0, slot = 0, prev = -1;
+    while (issued < nsteps) {
+        const int n = std::min(IMAG_CHUNK, nsteps - issued);
+        for (int j = 0; j < n; ++j) {
+            if (b->exec) {
+                GPE_CUDA(cudaGraphLaunch(b->exec, b->st));
+                b->replayed += b->graph_launches;
+            } else {
+                GPE_TRY(batch_issue_iteration<R>(b));
+            }
         }
+        issued += n;
+        if (issued >= nsteps) break;
+        GPE_CUDA(cudaMemsetAsync(b->d_running + slot, 0, sizeof(int), b->st));
+        for (gpe_handle* h : b->groups) {
+            k_any_running<<<1, 256, 0, b->st>>>(h->sc, h->nb, b->d_running + slot);
+            b->groups[0]->launches++;
+        }
+        GPE_CUDA(cudaMemcpyAsync(b->flag_host + slot, b->d_running + slot, sizeof(int), cudaMemcpyDeviceToHost, b->st));
+        GPE_CUDA(cudaEventRecord(b->flag_ev[slot], b->st));
+        if (prev >= 0) {
+            GPE_CUDA(cudaEventSynchronize(b->flag_ev[prev]));
+            if (!b->flag_host[prev]) break;
+        }
+        prev = slot;
+        slot ^= 1;
     }
     GPE_CUDA(cudaStreamSynchronize(b->st));
     GPE_CUDA(cudaGetLastError());
@@ -2038,6 +2089,10 @@ gpe_status gpe_batch_destroy(gpe_batch* b) {
     batch_drop_graph(b);
     if (b->stage_args) cudaFree(b->stage_args);
     if (b->bar) cudaFree(b->bar);
+    if (b->d_running) cudaFree(b->d_running);
+    if (b->flag_host) cudaFreeHost(b->flag_host);
+    for (cudaEvent_t e : b->flag_ev)
+        if (e) cudaEventDestroy(e);
     for (gpe_handle* h : b->groups) {
         free_all(h);
         delete h;
@@ -2124,6 +2179,14 @@ gpe_status gpe_batch_set_persistent(gpe_batch* b, int enable, unsigned int wait_
 }
 
 int gpe_batch_persistent(const gpe_batch* b) { return (b && b->persistent) ? 1 : 0; }
+
+gpe_status gpe_batch_persistent_info(const gpe_batch* b, long long* out) {
+    if (!b || !out) return fail(GPE_ERR_INVALID_ARG, "null argument");
+    const cudaError_t e = batch_stage_attributes(b->prec == GPE_C64 ? 8 : 16, out);
+    if (e != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("stage kernel attributes: ") + cudaGetErrorString(e));
+    out[8] = b->stage_grid;
+    return GPE_OK;
+}
 
 long long gpe_batch_kernel_launches(const gpe_batch* b) {
     if (!b) return 0;

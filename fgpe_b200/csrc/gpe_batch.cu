@@ -18,14 +18,14 @@ size_t batch_stage_smem(int esz) {
 bool batch_length_supported(int L) { return batch_length_ok(L); }
 
 template <typename R>
-static cudaError_t launch_stage(const BatchStage<R>& b, unsigned max_tiles, cudaStream_t st, int* grid_out) {
+static cudaError_t launch_stage(const BatchStage<R>& b, unsigned max_tiles, cudaStream_t st, BatchLaunchInfo* info) {
     const size_t smem = batch_stage_smem((int)sizeof(typename Cx<R>::T));
-    static std::atomic<unsigned long long> attr{0};
-    cudaError_t e = allow_smem(k_batch_stage<R>, smem, attr);
-    if (e != cudaSuccess) return e;
-    // CTAs per SM and SMs of each device, looked up once
+    // CTAs per SM and SMs of each device, looked up once; the dynamic shared
+    // memory is opted in whatever its size (the kernel's static arrays count
+    // against the 48 KB default too)
     constexpr int MAXDEV = 64;
     static std::atomic<int> cached[MAXDEV];
+    cudaError_t e;
     int dev = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     int per_sm = 0, nsm = 0;
@@ -34,6 +34,9 @@ static cudaError_t launch_stage(const BatchStage<R>& b, unsigned max_tiles, cuda
         per_sm = c & 0xffff;
         nsm = c >> 16;
     } else {
+        if ((e = cudaFuncSetAttribute(k_batch_stage<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+            cudaSuccess)
+            return e;
         if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
         if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_stage<R>, BATCH_THREADS, smem)) !=
             cudaSuccess)
@@ -41,7 +44,13 @@ static cudaError_t launch_stage(const BatchStage<R>& b, unsigned max_tiles, cuda
         if (dev >= 0 && dev < MAXDEV && per_sm > 0 && per_sm < 0x10000 && nsm < 0x8000)
             cached[dev].store(per_sm | (nsm << 16));
     }
-    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    if (info) {
+        info->per_sm = per_sm;
+        info->nsm = nsm;
+        info->smem = smem;
+        info->grid = 0;
+    }
+    if (per_sm < 1) return cudaErrorLaunchOutOfResources;
     // co-resident CTAs (the cooperative launch checks it), no more than the tiles
     unsigned grid = (unsigned)(per_sm * nsm);
     if (max_tiles < grid) grid = max_tiles > 0 ? max_tiles : 1;
@@ -55,15 +64,50 @@ static cudaError_t launch_stage(const BatchStage<R>& b, unsigned max_tiles, cuda
     at[0].val.cooperative = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    if (grid_out) *grid_out = (int)grid;
-    return cudaLaunchKernelEx(&cfg, k_batch_stage<R>, b);
+    if (info) info->grid = (int)grid;
+    e = cudaLaunchKernelEx(&cfg, k_batch_stage<R>, b);
+    if (e != cudaSuccess) cudaGetLastError();  // a refused launch leaves no error behind for later calls
+    return e;
 }
 
-cudaError_t launch_batch_stage(const BatchStage<float>& b, unsigned max_tiles, cudaStream_t st, int* grid) {
-    return launch_stage<float>(b, max_tiles, st, grid);
+template <typename R>
+static cudaError_t stage_attributes(long long* out) {
+    const size_t smem = batch_stage_smem((int)sizeof(typename Cx<R>::T));
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, k_batch_stage<R>);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_batch_stage<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+        cudaSuccess)
+        return e;
+    int dev = 0, nsm = 0, per_sm = 0, coop = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_stage<R>, BATCH_THREADS, smem)) !=
+        cudaSuccess)
+        return e;
+    out[0] = fa.numRegs;
+    out[1] = (long long)fa.sharedSizeBytes;
+    out[2] = fa.maxThreadsPerBlock;
+    out[3] = (long long)fa.localSizeBytes;
+    out[4] = per_sm;
+    out[5] = nsm;
+    out[6] = coop;
+    out[7] = (long long)smem;
+    return cudaSuccess;
 }
-cudaError_t launch_batch_stage(const BatchStage<double>& b, unsigned max_tiles, cudaStream_t st, int* grid) {
-    return launch_stage<double>(b, max_tiles, st, grid);
+
+cudaError_t batch_stage_attributes(int esz, long long* out) {
+    return esz == 8 ? stage_attributes<float>(out) : stage_attributes<double>(out);
+}
+
+cudaError_t launch_batch_stage(const BatchStage<float>& b, unsigned max_tiles, cudaStream_t st,
+                               BatchLaunchInfo* info) {
+    return launch_stage<float>(b, max_tiles, st, info);
+}
+cudaError_t launch_batch_stage(const BatchStage<double>& b, unsigned max_tiles, cudaStream_t st,
+                               BatchLaunchInfo* info) {
+    return launch_stage<double>(b, max_tiles, st, info);
 }
 
 }  // namespace gpe

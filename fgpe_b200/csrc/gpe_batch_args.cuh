@@ -45,11 +45,23 @@ struct BatchStage {
     unsigned wait_bound;                       // iterations a barrier wait may spin
 };
 
+// What a stage launch used: resident CTAs per SM, SMs, dynamic shared
+// memory, grid (0 when nothing was launched).
+struct BatchLaunchInfo {
+    int per_sm, nsm, grid;
+    size_t smem;
+};
+
 // Dynamic shared memory of the stage kernel and its launch (gpe_batch.cu):
-// grid = co-resident CTAs, at most max_tiles; *grid receives it.
+// grid = co-resident CTAs, at most max_tiles.
 size_t batch_stage_smem(int esz);
+// Resources of the stage kernel for fields of esz bytes: registers, static
+// shared memory, threads per CTA allowed, local memory per thread, resident
+// CTAs per SM, SMs, cooperative launch support, dynamic shared memory.
+cudaError_t batch_stage_attributes(int esz, long long* out);
 bool batch_length_supported(int L);
-cudaError_t launch_batch_stage(const BatchStage<float>& b, unsigned max_tiles, cudaStream_t st, int* grid);
-cudaError_t launch_batch_stage(const BatchStage<double>& b, unsigned max_tiles, cudaStream_t st, int* grid);
+cudaError_t launch_batch_stage(const BatchStage<float>& b, unsigned max_tiles, cudaStream_t st, BatchLaunchInfo* info);
+cudaError_t launch_batch_stage(const BatchStage<double>& b, unsigned max_tiles, cudaStream_t st,
+                               BatchLaunchInfo* info);
 
 }  // namespace gpe

@@ -239,6 +239,13 @@ __device__ void finalize_scalars(const PassArgs<R>& a, DevScalars* sc, const dou
     }
 }
 
+// Block-reduction scratch: one array per kernel, however many tile bodies
+// (lengths, kinds) the kernel inlines.
+__device__ __forceinline__ DD* reduce_scratch() {
+    __shared__ DD red[32 * MAXQ];
+    return red;
+}
+
 // bidx: this tile's partial slot; nblk: the tiles of the instance (the last
 // of them to arrive finalises).
 template <typename R, int NQ>
@@ -530,8 +537,10 @@ __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const typen
             return;
         } else if constexpr (EPI == EPI_ADJ) {
             // Reverse of one stage of the real-time RK4 step with
-            // f(psi) = -i h(psi), h = T + W + g|psi|^2 (one component):
-            //   jt = J^T mu = i (T mu + (W.re + 2 g |psi_s|^2) mu - i W.im mu) - i g psi_s^2 conj(mu)
+            // f(psi) = -i h(psi), h = T + W + g|psi|^2 + Phi[|psi|^2] (one
+            // component; Phi = 0 without a k-space interaction):
+            //   jt = J^T mu = i (T mu + (W.re + 2 g |psi_s|^2 + Phi[|psi_s|^2]) mu - i W.im mu)
+            //                 - i g psi_s^2 conj(mu) + 2 Phi[Im(conj(mu) psi_s)] psi_s
             //   q  += Im(conj(mu) psi_s)           (control-gradient density)
             //   stage 4: acc = lambda + jt; 3, 2: acc += jt; 1: lambda <- acc + jt
             //   next mu = c_re * lambda + c_im * jt   (stages 4, 3, 2)
@@ -539,13 +548,22 @@ __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const typen
             const C Tm = T[0];
             const R g = hc.g_mu;
             const R n2 = ps.x * ps.x + ps.y * ps.y;
-            const R aw = V[0].x + 2 * g * n2;
+            R aw = V[0].x + 2 * g * n2;
+            // k-space interaction (dipolar, soft core): phi = Phi[|psi_s|^2]
+            // acts like the potential; its Jacobian psi_s Phi[2 Re(conj(psi_s) d)]
+            // transposes to 2 Phi[Im(conj(mu) psi_s)] psi_s (Phi symmetric)
+            if (NF > 1 && a.dens) aw += phi;
             const R Ar = Tm.x + aw * mu.x + V[0].y * mu.y;
             const R Ai = Tm.y + aw * mu.y - V[0].y * mu.x;
             const R s2r = ps.x * ps.x - ps.y * ps.y, s2i = 2 * ps.x * ps.y;
             const R Br = s2r * mu.x + s2i * mu.y;
             const R Bi = s2i * mu.x - s2r * mu.y;
-            const C jt = mk(-Ai + g * Bi, Ar - g * Br);
+            C jt = mk(-Ai + g * Bi, Ar - g * Br);
+            if (NF > 1 && a.dens) {
+                const R pr = 2 * v[NF - 1].y;
+                jt.x += pr * ps.x;
+                jt.y += pr * ps.y;
+            }
             R q = mu.x * ps.y - mu.y * ps.x;
             R* qf = reinterpret_cast<R*>(a.out[1]);
             const int stage = a.stage;
@@ -766,6 +784,14 @@ __device__ __forceinline__ void xpass_tile(const PassArgs<R>& a, int rows, unsig
             for (int f = 0; f < NF; ++f) {
                 if (f < npsi) {
                     v[f][e] = valid ? load_psi<R>(a, ps, f, gi, cur) : mk((R)0, (R)0);
+                } else if (a.epi == EPI_ADJ) {
+                    // adjoint chain: the stage argument's density |psi_s|^2 and
+                    // Im(conj(mu) psi_s), the two real inputs of the k-space
+                    // interaction's Jacobian, as one complex field (the table
+                    // is real and even in k, so the parts stay apart)
+                    const C p = v[0][e];
+                    const C q = valid ? a.buf[0][0][gi] : mk((R)0, (R)0);
+                    v[f][e] = mk(q.x * q.x + q.y * q.y, p.x * q.y - p.y * q.x);
                 } else {
                     const C p = v[0][e];
                     v[f][e] = mk(p.x * p.x + p.y * p.y, (R)0);
@@ -827,8 +853,7 @@ __device__ __forceinline__ void xpass_tile(const PassArgs<R>& a, int rows, unsig
         }
         if constexpr (kind_reduces<KIND>()) {
             if (epi_reduces(a)) {
-                __shared__ DD red[32 * MAXQ];
-                reduce_and_finalize<R, MAXQ>(a, ip, acc, red, tile, ntiles);
+                reduce_and_finalize<R, MAXQ>(a, ip, acc, reduce_scratch(), tile, ntiles);
             }
         }
     }
@@ -1168,7 +1193,7 @@ cudaError_t launch_xpass(const PassArgs<R>& a, int rows, size_t smem, cudaStream
     if (kind == XK_RK && a.want_obs && a.stage == 4) kind = XK_RKO;
     else if (kind == XK_RK && a.fuse_fwd) kind = XK_RKF;
     if (kind == XK_ADJ) {
-        if constexpr (NF == 1 && H::builtin) return launch_xpass_kind<R, L, NF, XK_ADJ, H>(a, rows, smem, st);
+        if constexpr (NF <= 2 && H::builtin) return launch_xpass_kind<R, L, NF, XK_ADJ, H>(a, rows, smem, st);
         return cudaErrorNotSupported;
     }
     switch (kind) {

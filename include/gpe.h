@@ -251,12 +251,15 @@ gpe_status gpe_dsz_dt(gpe_handle* h, double* out);
 gpe_status gpe_fft(gpe_handle* h, int comp, int sign);
 
 /* ---- optimal-control gradient (no counterpart in the reference) ------------
- * Real-time RK4 (the gpe_step_real scheme, one component, GPE_HAM_BEC) where
- * step n uses the potential W_n = V + sum_k u[n*nctrl + k] G_k, and the
- * final-state infidelity L = 1 - |o|^2, o = sum conj(target) psi(T) DV.
+ * Real-time RK4 (the gpe_step_real scheme, one component, GPE_HAM_BEC,
+ * GPE_HAM_DIPOLAR or GPE_HAM_SOFT) where step n uses the potential
+ * W_n = V + sum_k u[n*nctrl + k] G_k, and the final-state infidelity
+ * L = 1 - |o|^2, o = sum conj(target) psi(T) DV.
  * The gradient dL/du is the discrete adjoint of the RK4 step: each stage's
- * transpose Jacobian J^T mu = i (T + W + 2g|psi|^2) mu - i g psi^2 conj(mu)
- * runs through the same fused FFT passes; states are recomputed from
+ * transpose Jacobian J^T mu = i (T + W + 2g|psi|^2 + Phi[|psi|^2]) mu
+ * - i g psi^2 conj(mu) + 2 Phi[Im(conj(mu) psi)] psi (Phi: the k-space
+ * interaction, 0 for GPE_HAM_BEC) runs through the same fused FFT passes,
+ * both real densities of Phi in one transformed field; states are recomputed from
  * checkpoints every checkpoint_every steps (memory: about
  * nsteps/checkpoint_every + checkpoint_every + 8 fields). */
 /* nctrl (1..64) real basis functions, host array nctrl x N (FP64). */
@@ -307,6 +310,11 @@ long long  gpe_batch_kernel_launches(const gpe_batch* b);
  * process). */
 gpe_status gpe_batch_set_persistent(gpe_batch* b, int enable, unsigned int wait_bound);
 int        gpe_batch_persistent(const gpe_batch* b);
+/* Resources of the batch's persistent stage kernel, out[0..8]: registers per
+ * thread, static shared memory (B), threads per CTA allowed, local memory per
+ * thread (B), resident CTAs per SM, SMs, cooperative launch supported (0/1),
+ * dynamic shared memory (B), CTAs of the last stage launch. */
+gpe_status gpe_batch_persistent_info(const gpe_batch* b, long long* out);
 
 /* ---- user Hamiltonian plugins ------------------------------------------------
  * A plugin is a shared library compiled from the user's .cu file with

@@ -15,9 +15,18 @@ the Laplace operator of src/baseHamiltonian.cu:86-96 / src/parallel.cu:194-205):
 
 Loss: L = 1 - |o|^2, o = sum conj(psi_target) psi_T DV.
 
+With a k-space interaction (the dipolar term of GPE_HAM_DIPOLAR without the
+cut-off: the reference's DipoleDipoleInteraction kernel, src/parallel.cu:326-352)
+h gains Phi[|psi|^2] psi, Phi[n] = IFFT[V~(k) FFT n] (real for real n: V~ is
+real and even in k).
+
 Adjoint (gradients as complex numbers d/dRe + i d/dIm, real inner product
-Re sum conj(a) b):  J^T mu = i (T mu + W mu + 2 g |psi|^2 mu) - i g psi^2 conj(mu)
-with g = 4 pi a; dL/du[n, k] = sum_s sum_x G_k(x) Im(conj(lam_ks(x)) psi_s(x)).
+Re sum conj(a) b):
+    J^T mu = i (T mu + (W + 2 g |psi|^2 + Phi[|psi|^2]) mu) - i g psi^2 conj(mu)
+             + 2 Phi[Im(conj(mu) psi)] psi
+(W.imag enters as - i W.imag mu inside the bracket) with g = 4 pi a; the last
+term is the transpose of psi Phi[2 Re(conj(psi) d)], Phi being symmetric.
+dL/du[n, k] = sum_s sum_x G_k(x) Im(conj(lam_ks(x)) psi_s(x)).
 """
 from __future__ import annotations
 
@@ -27,8 +36,9 @@ LAP = 19.739208802  # src/parallel.cu:199
 PI_REF = 3.141592653589793
 
 
-def k_squared(cfg):
-    """k^2 on the grid (src/baseHamiltonian.cu:53-82 with the odd-N formula)."""
+def k_axes(cfg):
+    """k axes in cycles per length (src/baseHamiltonian.cu:53-82 with the
+    odd-N formula); axes beyond the dimension are zero."""
     ks = []
     for d, n in enumerate((cfg.nx, cfg.ny, cfg.nz)):
         dx = cfg.dx[d]
@@ -39,12 +49,33 @@ def k_squared(cfg):
             k[i] = i * dk if i <= n // 2 else -kmax + (i - n // 2) * dk
         zero = (cfg.dim == 1 and d > 0) or (cfg.dim == 2 and d == 2)
         ks.append(np.zeros(n) if zero else k)
-    kx, ky, kz = ks
+    return ks
+
+
+def k_squared(cfg):
+    """k^2 on the grid."""
+    kx, ky, kz = k_axes(cfg)
     return kz[:, None, None] ** 2 + ky[None, :, None] ** 2 + kx[None, None, :] ** 2
 
 
+def dipolar_table(cfg):
+    """V~(k) = 12 pi a_dd ((k.d)^2 / k^2 - 1/3), 0 for |k| < 1e-6, a_dd =
+    prms[6], d = prms[7:10] normalised (src/parallel.cu:326-352); only
+    without the real-space cut-off (prms[10] = 0)."""
+    if cfg.prms[10] != 0:
+        raise ValueError("dipolar_table restates the kernel without the cut-off (prms[10] = 0)")
+    kx, ky, kz = k_axes(cfg)
+    KZ, KY, KX = np.meshgrid(kz, ky, kx, indexing="ij")
+    d = np.array([cfg.prms[7], cfg.prms[8], cfg.prms[9]], dtype=np.float64)
+    d = d / np.linalg.norm(d)
+    kk = np.sqrt(KX ** 2 + KY ** 2 + KZ ** 2)
+    kd = KX * d[0] + KY * d[1] + KZ * d[2]
+    safe = np.where(kk < 1e-6, 1.0, kk)
+    return np.where(kk < 1e-6, 0.0, 12.0 * PI_REF * cfg.prms[6] * ((kd / safe) ** 2 - 1.0 / 3.0))
+
+
 class ControlProblem:
-    def __init__(self, cfg, V0, G, psi0, target):
+    def __init__(self, cfg, V0, G, psi0, target, vtab=None):
         self.cfg = cfg
         self.N = cfg.nx * cfg.ny * cfg.nz
         self.shape = (cfg.nz, cfg.ny, cfg.nx)
@@ -57,6 +88,13 @@ class ControlProblem:
         self.g = 4 * PI_REF * cfg.prms[2]
         self.dt = cfg.dt
         self.DV = cfg.dx[0] * cfg.dx[1] * cfg.dx[2]
+        self.vtab = None if vtab is None else np.asarray(vtab, np.float64).reshape(self.shape)
+
+    def Phi(self, n):
+        """The k-space interaction's potential of a real density (0 without one)."""
+        if self.vtab is None:
+            return 0.0
+        return np.real(np.fft.ifftn(self.vtab * np.fft.fftn(n)))
 
     def T(self, p):
         return np.fft.ifftn(self.scale * self.K2 * np.fft.fftn(p)) * self.N
@@ -65,7 +103,8 @@ class ControlProblem:
         return self.V0 + np.tensordot(u_n, self.G, axes=(0, 0))
 
     def f(self, p, W):
-        return -1j * (self.T(p) + (W.real + self.g * np.abs(p) ** 2) * p + 1j * W.imag * p)
+        n = np.abs(p) ** 2
+        return -1j * (self.T(p) + (W.real + self.g * n + self.Phi(n)) * p + 1j * W.imag * p)
 
     def step(self, p, W, keep=False):
         dt = self.dt
@@ -80,8 +119,12 @@ class ControlProblem:
         return (nxt, (p, pa, pb, pc)) if keep else nxt
 
     def JT(self, mu, p, W):
-        return 1j * (self.T(mu) + (W.real + 2 * self.g * np.abs(p) ** 2) * mu - 1j * W.imag * mu) \
+        n = np.abs(p) ** 2
+        jt = 1j * (self.T(mu) + (W.real + 2 * self.g * n + self.Phi(n)) * mu - 1j * W.imag * mu) \
             - 1j * self.g * p ** 2 * np.conj(mu)
+        if self.vtab is not None:
+            jt = jt + 2.0 * self.Phi(np.imag(np.conj(mu) * p)) * p
+        return jt
 
     def forward(self, u):
         p = self.psi0.copy()

@@ -112,6 +112,32 @@ def test_batch_convergence_per_instance(gpu):
     assert len(set(want)) > 1  # the instances converge at different iterations
 
 
+def test_batch_stops_issuing_after_every_instance_converged(gpu):
+    """A call asked for far more iterations than convergence needs issues at
+    most a few chunks (64 iterations each) past the last instance's
+    convergence."""
+    import torch
+    cfgs, traps = sweep_configs(C64, IMAG_RK4, eps=1e-5, dt=5e-3)
+    stream = torch.cuda.Stream()
+    with Batch(cfgs) as b:
+        b.set_stream(stream.cuda_stream)
+        for i, c in enumerate(cfgs):
+            b.set_vext(i, traps[i])
+            b.set_psi(i, initial(c, 10 + i))
+        b.step_imag(1)  # graph capture
+        l0 = b.launches
+        b.step_imag(2)
+        per_iter = (b.launches - l0 - len(set((c.nx, c.ny) for c in cfgs))) // 2  # minus the per-call resets
+        for i, c in enumerate(cfgs):
+            b.set_vext(i, traps[i])
+            b.set_psi(i, initial(c, 10 + i))
+        l1 = b.launches
+        it, cv = b.step_imag(1000000)
+        assert cv.all() and it.max() < 3000
+        issued = (b.launches - l1) / per_iter
+        assert it.max() <= issued <= it.max() + 3 * 64, (issued, it.max())
+
+
 def test_batch_rejects_mixed_settings(gpu):
     a = make_config((32, 32, 1), (6.0, 6.0, 1.0), precision=C64, g=10.0, imag_scheme=IMAG_RK4)
     b = make_config((32, 32, 1), (6.0, 6.0, 1.0), precision=C128, g=10.0, imag_scheme=IMAG_RK4)
