@@ -590,10 +590,11 @@ def run_sweep(args):
     # autotune every geometry group in place: per group the default and the
     # tuned microseconds per iteration, measured on the same work
     tune_rep = None if args.no_tune else b.tune(os.path.join("/tmp", f"gpe_tune_{os.getpid()}.jsonl"))
-    def timed(persistent):
+    def timed(mode):
         """W warm-up and K timed iterations of every instance from the seeded
-        start, under per-group or persistent stage launches."""
-        b.set_persistent(persistent)
+        start under one launch mode (per group; one cooperative launch per
+        stage; one launch per pass over all groups)."""
+        b.set_launch_mode(mode)
         for i, (c, V, p, *_ ) in enumerate(inst):
             b.set_vext(i, V)
             b.set_psi(i, p)
@@ -608,13 +609,16 @@ def run_sweep(args):
         return e0.elapsed_time(e1), it, cv, b.launches - l0
 
     # both launch modes on the same work; the faster one is the headline
-    modes = {"per_group": timed(False)}
-    try:
-        modes["persistent"] = timed(True)
-    except gp.GPEError as e:
-        modes["persistent"] = str(e)
+    mode_ids = {"per_group": gp.BATCH_PER_GROUP, "persistent": gp.BATCH_PERSISTENT, "grouped": gp.BATCH_GROUPED}
+    modes = {}
+    with Clocks(torch.cuda.current_device()) as clk:
+        for name, mid in mode_ids.items():
+            try:
+                modes[name] = timed(mid)
+            except gp.GPEError as e:
+                modes[name] = str(e)
     best = min((k for k in modes if not isinstance(modes[k], str)), key=lambda k: modes[k][0])
-    b.set_persistent(best == "persistent")
+    b.set_launch_mode(mode_ids[best])
     ms, it, cv, launches = modes[best]
     launch_modes = {k: (v if isinstance(v, str) else
                         {"ms_per_step": round(v[0] / K, 4), "launches_per_iteration": round(v[3] / K, 2),
@@ -685,7 +689,7 @@ def run_sweep(args):
                          "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": round(alg_bytes / (ms / 1e3) / 1e9 / peak, 4), "traffic": None,
                          "model": "45 F per RK4 imaginary iteration, F = N*8 B"},
-            "tuning": tuning_summary(tune_rep, inst), "launch_modes": launch_modes,
+            "tuning": tuning_summary(tune_rep, inst), "launch_modes": launch_modes, "clocks": clk.summary(),
             "gpu_launches": launches, "convergence": conv,
             "cpu_baseline": sweep_cpu_leg(everything, stream)}
     if world > 1:

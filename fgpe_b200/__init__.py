@@ -31,6 +31,11 @@ NO_HAMIL_PARAMS = 32
 C128, C64 = 0, 1
 HAM_BEC, HAM_BEC2, HAM_TEMPLATE, HAM_DIPOLAR, HAM_SOFT, HAM_USER = 0, 1, 2, 3, 4, 5
 IMAG_HEAVYBALL, IMAG_RK4 = 0, 1
+# gpe_batch_mode (include/gpe.h)
+BATCH_PER_GROUP, BATCH_PERSISTENT, BATCH_GROUPED = 0, 1, 2
+# gpe_lattice (include/gpe.h): Psi::force*Lattice seeds
+LATTICE_1D, LATTICE_2D_TRIANGULAR, LATTICE_2D_SQUARE, LATTICE_3D_HEX, LATTICE_3D_FCC, LATTICE_3D_BCC, \
+    LATTICE_3D_SC = 1, 2, 3, 4, 5, 6, 7
 ABI_VERSION = 1
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported", 3: "CUDA error",
@@ -88,6 +93,8 @@ def lib() -> ctypes.CDLL:
         "gpe_get_psi": (c_int, [H, c_int, P]),
         "gpe_set_vext": (c_int, [H, c_int, P]),
         "gpe_set_psi_device": (c_int, [H, c_int, c_void_p]),
+        "gpe_imprint_vortex_tube": (c_int, [H, c_int, c_double]),
+        "gpe_seed_lattice": (c_int, [H, c_int, c_int, c_double, c_double, P, c_double, c_double]),
         "gpe_get_psi_device": (c_int, [H, c_int, c_void_p]),
         "gpe_step_real": (c_int, [H, c_int, c_int, P]),
         "gpe_step_imag": (c_int, [H, c_int, c_int, POINTER(c_int), POINTER(c_int)]),
@@ -123,6 +130,8 @@ def lib() -> ctypes.CDLL:
         "gpe_batch_groups": (c_int, [H]),
         "gpe_batch_set_persistent": (c_int, [H, c_int, ctypes.c_uint]),
         "gpe_batch_persistent": (c_int, [H]),
+        "gpe_batch_set_launch_mode": (c_int, [H, c_int, ctypes.c_uint]),
+        "gpe_batch_launch_mode": (c_int, [H]),
         "gpe_batch_persistent_info": (c_int, [H, POINTER(c_longlong)]),
         "gpe_get_pass_variants": (c_int, [H, POINTER(c_int)]),
         "gpe_set_pass_variants": (c_int, [H, POINTER(c_int)]),
@@ -289,6 +298,19 @@ class Solver:
 
     def get_psi_device(self, comp: int, ptr: int) -> None:
         _check(lib().gpe_get_psi_device(self._h, comp, c_void_p(ptr)))
+
+    def imprint_vortex_tube(self, comp: int, ncirc: float) -> None:
+        """psi *= exp(i ncirc 2 pi x / (2 xmax_x)) on the device (gpe_imprint_vortex_tube)."""
+        _check(lib().gpe_imprint_vortex_tube(self._h, comp, float(ncirc)))
+
+    def seed_lattice(self, comp: int, lattice: int, amp: float, k: float, off=(0.0, 0.0, 0.0),
+                     seed_npart: float = 1.0, norm_npart: float = 1.0) -> None:
+        """Add a Psi::force*Lattice seed and renormalise, on the device (gpe_seed_lattice)."""
+        o = np.ascontiguousarray(off, dtype=np.float64)
+        if o.size != 3:
+            raise ValueError("off needs 3 offsets")
+        _check(lib().gpe_seed_lattice(self._h, comp, int(lattice), float(amp), float(k), _dp(o), float(seed_npart),
+                                      float(norm_npart)))
 
     def step_real(self, first_iteration: int, nsteps: int, want_obs: bool = False):
         if want_obs:
@@ -493,6 +515,14 @@ class Batch:
         (gpe_batch_set_persistent); wait_bound: iterations a grid-barrier
         wait may spin, 0 for the default (about a second)."""
         _check(lib().gpe_batch_set_persistent(self._h, 1 if enable else 0, int(wait_bound)))
+
+    def set_launch_mode(self, mode: int, wait_bound: int = 0) -> None:
+        """BATCH_PER_GROUP, BATCH_PERSISTENT or BATCH_GROUPED (gpe_batch_set_launch_mode)."""
+        _check(lib().gpe_batch_set_launch_mode(self._h, int(mode), int(wait_bound)))
+
+    @property
+    def launch_mode(self) -> int:
+        return int(lib().gpe_batch_launch_mode(self._h))
 
     @property
     def persistent(self) -> bool:

@@ -12,6 +12,7 @@
 
 #include "../../include/gpe.h"
 #include "gpe_dispatch.cuh"
+#include "gpe_init.cuh"
 #include "gpe_sizes.h"
 
 using namespace gpe;
@@ -1490,6 +1491,60 @@ gpe_status gpe_get_psi_device(gpe_handle* h, int comp, void* dev_c128) {
     return GPE_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Runs f on a complex128 device copy of component comp's psi, then sets psi
+// from it (the precision's rounding and low part as gpe_set_psi_device).
+template <class F>
+gpe_status on_c128_psi(gpe_handle* h, int comp, F f) {
+    GPE_TRY(check_handle(h));
+    GPE_TRY(check_comp(h, comp));
+    void* buf = nullptr;
+    double* part = nullptr;
+    gpe_status s = GPE_OK;
+    if (cudaMalloc(&buf, 16 * h->N) != cudaSuccess || cudaMalloc((void**)&part, seed_partials_bytes()) != cudaSuccess)
+        s = fail(GPE_ERR_OUT_OF_MEMORY, "seed work buffers");
+    if (s == GPE_OK) s = gpe_get_psi_device(h, comp, buf);
+    if (s == GPE_OK) {
+        SeedGrid g;
+        const int n[3] = {h->nx, h->ny, h->nz};
+        for (int d = 0; d < 3; ++d) {
+            g.n[d] = n[d];
+            g.xmax[d] = h->cfg.xmax[d];
+            g.dx[d] = h->cfg.dx[d];
+        }
+        const cudaError_t e = f((double2*)buf, g, part);
+        if (e != cudaSuccess) s = fail(GPE_ERR_CUDA, std::string("seed kernels: ") + cudaGetErrorString(e));
+    }
+    if (s == GPE_OK) s = gpe_set_psi_device(h, comp, buf);
+    cudaStreamSynchronize(h->st);
+    if (buf) cudaFree(buf);
+    if (part) cudaFree(part);
+    return s;
+}
+
+}  // namespace
+
+extern "C" {
+
+gpe_status gpe_imprint_vortex_tube(gpe_handle* h, int comp, double ncirc) {
+    return on_c128_psi(h, comp, [&](double2* p, const SeedGrid& g, double*) {
+        return imprint_vortex_tube_c128(p, g, ncirc, h->st);
+    });
+}
+
+gpe_status gpe_seed_lattice(gpe_handle* h, int comp, int lattice, double amp, double k, const double* off,
+                            double seed_npart, double norm_npart) {
+    if (lattice < GPE_LATTICE_1D || lattice > GPE_LATTICE_3D_SC) return fail(GPE_ERR_INVALID_ARG, "unknown lattice");
+    if (!off) return fail(GPE_ERR_INVALID_ARG, "null offsets");
+    if (!(seed_npart > 0) || !(norm_npart > 0)) return fail(GPE_ERR_INVALID_ARG, "particle numbers must be > 0");
+    return on_c128_psi(h, comp, [&](double2* p, const SeedGrid& g, double* part) {
+        return seed_lattice_c128(p, g, lattice, amp, k, off, seed_npart, norm_npart, part, h->st);
+    });
+}
+
 gpe_status gpe_set_vext(gpe_handle* h, int comp, const double* host_c128) {
     GPE_TRY(check_handle(h));
     GPE_TRY(check_comp(h, comp));
@@ -1748,7 +1803,7 @@ struct gpe_batch {
     long long replayed = 0;              // kernels run by graph replays
     // persistent stage launches (gpe_batch_set_persistent): one cooperative
     // launch per RK4 stage for every group
-    bool persistent = false;
+    int mode = GPE_BATCH_PER_GROUP;      // gpe_batch_set_launch_mode
     unsigned wait_bound = 0;             // iterations a grid-barrier wait may spin
     void* stage_args = nullptr;          // device PassArgs [4 stages][3 phases][BATCH_MAX_GROUPS]
     GridBar* bar = nullptr;
@@ -1898,9 +1953,26 @@ gpe_status batch_issue_stages(gpe_batch* b) {
     return GPE_OK;
 }
 
+// GPE_BATCH_GROUPED: per stage three launches (x forward, strided, x
+// inverse), each over the tiles of every instance of every group.
+template <typename R>
+gpe_status batch_issue_phases(gpe_batch* b) {
+    for (int s = 1; s <= 4; ++s) {
+        unsigned max_tiles = 0;
+        const BatchStage<R> d = batch_stage_desc<R>(b, s, &max_tiles);
+        for (int ph = 0; ph < 3; ++ph) {
+            const cudaError_t e = launch_batch_phase(d, ph, b->st);
+            if (e != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("batch phase launch: ") + cudaGetErrorString(e));
+            b->stage_launches++;
+        }
+    }
+    return GPE_OK;
+}
+
 template <typename R>
 gpe_status batch_issue_iteration(gpe_batch* b) {
-    if (b->persistent) return batch_issue_stages<R>(b);
+    if (b->mode == GPE_BATCH_PERSISTENT) return batch_issue_stages<R>(b);
+    if (b->mode == GPE_BATCH_GROUPED) return batch_issue_phases<R>(b);
     for (gpe_handle* h : b->groups) GPE_TRY(imag_issue<R>(h, 0, 1));
     return GPE_OK;
 }
@@ -1965,7 +2037,7 @@ gpe_status batch_flags(gpe_batch* b) {
 template <typename R>
 gpe_status batch_step_imag_t(gpe_batch* b, int nsteps, int* iters_done, int* converged) {
     for (gpe_handle* h : b->groups) GPE_TRY(imag_prepare<R>(h));
-    if (b->persistent) GPE_CUDA(cudaMemsetAsync(b->bar, 0, sizeof(GridBar), b->st));
+    if (b->mode == GPE_BATCH_PERSISTENT) GPE_CUDA(cudaMemsetAsync(b->bar, 0, sizeof(GridBar), b->st));
     GPE_TRY(batch_capture<R>(b));
     GPE_TRY(batch_flags(b));
     int issued = 0, slot = 0, prev = -1;
@@ -1997,7 +2069,7 @@ gpe_status batch_step_imag_t(gpe_batch* b, int nsteps, int* iters_done, int* con
     }
     GPE_CUDA(cudaStreamSynchronize(b->st));
     GPE_CUDA(cudaGetLastError());
-    if (b->persistent) {
+    if (b->mode == GPE_BATCH_PERSISTENT) {
         GridBar bar;
         GPE_CUDA(cudaMemcpy(&bar, b->bar, sizeof(bar), cudaMemcpyDeviceToHost));
         if (bar.status == GPE_ERR_TIMEOUT)
@@ -2163,22 +2235,30 @@ gpe_status gpe_batch_imag_state(gpe_batch* b, int inst, double* out) {
     return GPE_OK;
 }
 
-gpe_status gpe_batch_set_persistent(gpe_batch* b, int enable, unsigned int wait_bound) {
+gpe_status gpe_batch_set_launch_mode(gpe_batch* b, int mode, unsigned int wait_bound) {
     if (!b) return fail(GPE_ERR_INVALID_ARG, "null batch");
-    if (enable) {
+    if (mode != GPE_BATCH_PER_GROUP && mode != GPE_BATCH_PERSISTENT && mode != GPE_BATCH_GROUPED)
+        return fail(GPE_ERR_INVALID_ARG, "unknown batch launch mode");
+    if (mode != GPE_BATCH_PER_GROUP) {
         const std::string why = batch_persistent_reason(b);
-        if (!why.empty()) return fail(GPE_ERR_UNSUPPORTED, "persistent batch launch: " + why);
+        if (!why.empty()) return fail(GPE_ERR_UNSUPPORTED, "all-group batch launches: " + why);
         GPE_CUDA(cudaStreamSynchronize(b->st));
         GPE_TRY(b->prec == GPE_C64 ? batch_build_stages<float>(b) : batch_build_stages<double>(b));
     }
     batch_drop_graph(b);  // the captured launches carry the old choice and bound
-    b->persistent = enable != 0;
+    b->mode = mode;
     b->wait_bound = wait_bound;
     b->use_graph = true;
     return GPE_OK;
 }
 
-int gpe_batch_persistent(const gpe_batch* b) { return (b && b->persistent) ? 1 : 0; }
+int gpe_batch_launch_mode(const gpe_batch* b) { return b ? b->mode : GPE_BATCH_PER_GROUP; }
+
+gpe_status gpe_batch_set_persistent(gpe_batch* b, int enable, unsigned int wait_bound) {
+    return gpe_batch_set_launch_mode(b, enable ? GPE_BATCH_PERSISTENT : GPE_BATCH_PER_GROUP, wait_bound);
+}
+
+int gpe_batch_persistent(const gpe_batch* b) { return (b && b->mode == GPE_BATCH_PERSISTENT) ? 1 : 0; }
 
 gpe_status gpe_batch_persistent_info(const gpe_batch* b, long long* out) {
     if (!b || !out) return fail(GPE_ERR_INVALID_ARG, "null argument");

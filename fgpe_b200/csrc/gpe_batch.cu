@@ -70,6 +70,35 @@ static cudaError_t launch_stage(const BatchStage<R>& b, unsigned max_tiles, cuda
     return e;
 }
 
+template <typename R, int PHASE>
+static cudaError_t launch_phase_k(const BatchStage<R>& b, cudaStream_t st) {
+    const size_t smem = batch_stage_smem((int)sizeof(typename Cx<R>::T));
+    static std::atomic<unsigned long long> attr{0};
+    cudaError_t e = allow_smem(k_batch_phase<R, PHASE>, smem, attr);
+    if (e != cudaSuccess) return e;
+    const unsigned tiles = PHASE == 1 ? b.sstart[b.ngroups] : b.xstart[b.ngroups];
+    if (tiles == 0) return cudaSuccess;
+    e = launch_pass(k_batch_phase<R, PHASE>, tiles, 1u, (unsigned)BATCH_THREADS, smem, st, b);
+    if (e != cudaSuccess) cudaGetLastError();
+    return e;
+}
+
+template <typename R>
+static cudaError_t launch_phase(const BatchStage<R>& b, int phase, cudaStream_t st) {
+    switch (phase) {
+        case 0: return launch_phase_k<R, 0>(b, st);
+        case 1: return launch_phase_k<R, 1>(b, st);
+        default: return launch_phase_k<R, 2>(b, st);
+    }
+}
+
+cudaError_t launch_batch_phase(const BatchStage<float>& b, int phase, cudaStream_t st) {
+    return launch_phase<float>(b, phase, st);
+}
+cudaError_t launch_batch_phase(const BatchStage<double>& b, int phase, cudaStream_t st) {
+    return launch_phase<double>(b, phase, st);
+}
+
 template <typename R>
 static cudaError_t stage_attributes(long long* out) {
     const size_t smem = batch_stage_smem((int)sizeof(typename Cx<R>::T));

@@ -88,6 +88,66 @@ __host__ __device__ constexpr int batch_min_blocks() {
     return sizeof(R) == 4 ? 2 : 1;
 }
 
+// Tile t of phase A (x forward: stage-state prologue + x transform).
+template <typename R>
+__device__ __forceinline__ void batch_tile_a(const BatchStage<R>& b, unsigned t, unsigned char* smem_raw) {
+    const int ng = b.ngroups;
+    const int g = batch_group_of(b.xstart, ng, t);
+    const unsigned local = t - b.xstart[g], inst = local / b.xt[g], tile = local % b.xt[g];
+    const PassArgs<R>& a = b.args[g];
+    switch (b.lx[g]) {
+#define GPE_BATCH_XF(L)                                                              \
+    case L:                                                                          \
+        xpass_tile<R, L, 1, XK_FWD>(a, batch_rows(L), tile, inst, b.xt[g], smem_raw); \
+        break;
+        GPE_BATCH_LENGTHS(GPE_BATCH_XF)
+#undef GPE_BATCH_XF
+        default:
+            break;
+    }
+}
+
+// Tile t of phase B (y forward * k-space * inverse).
+template <typename R>
+__device__ __forceinline__ void batch_tile_b(const BatchStage<R>& b, unsigned t, unsigned char* smem_raw) {
+    const int ng = b.ngroups;
+    const int g = batch_group_of(b.sstart, ng, t);
+    const unsigned local = t - b.sstart[g], inst = local / b.st[g], tile = local % b.st[g];
+    const PassArgs<R>& a = b.args[BATCH_MAX_GROUPS + g];
+    switch (b.ly[g]) {
+#define GPE_BATCH_S(L)                                                        \
+    case L:                                                                   \
+        spass_tile<R, L, 1, batch_rows(L)>(a, b.ntx[g], tile, inst, smem_raw); \
+        break;
+        GPE_BATCH_LENGTHS(GPE_BATCH_S)
+#undef GPE_BATCH_S
+        default:
+            break;
+    }
+}
+
+// Tile t of phase C (x inverse with the RK4 imaginary-time epilogue and the
+// per-instance reductions).
+template <typename R>
+__device__ __forceinline__ void batch_tile_c(const BatchStage<R>& b, unsigned t, unsigned char* smem_raw) {
+    const int ng = b.ngroups;
+    const int g = batch_group_of(b.xstart, ng, t);
+    const unsigned local = t - b.xstart[g], inst = local / b.xt[g], tile = local % b.xt[g];
+    const PassArgs<R>& a = b.args[2 * BATCH_MAX_GROUPS + g];
+    switch (b.lx[g]) {
+#define GPE_BATCH_XI(L)                                                              \
+    case L:                                                                          \
+        xpass_tile<R, L, 1, XK_RKI>(a, batch_rows(L), tile, inst, b.xt[g], smem_raw); \
+        break;
+        GPE_BATCH_LENGTHS(GPE_BATCH_XI)
+#undef GPE_BATCH_XI
+        default:
+            break;
+    }
+}
+
+// One RK4 stage (imaginary time) of every instance of every group: the three
+// phases in one cooperative launch, a bounded grid barrier between them.
 template <typename R>
 __global__ void __launch_bounds__(BATCH_THREADS, batch_min_blocks<R>()) k_batch_stage(BatchStage<R> b) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -95,59 +155,39 @@ __global__ void __launch_bounds__(BATCH_THREADS, batch_min_blocks<R>()) k_batch_
     // a wait of an earlier stage gave up: the barrier counts are stale, so
     // no CTA takes part in this launch
     if (ld_volatile_i(&b.bar->status) != 0) return;
-    // phase A: x forward (stage-state prologue + x transform)
     for (unsigned t = blockIdx.x; t < b.xstart[ng]; t += gridDim.x) {
-        const int g = batch_group_of(b.xstart, ng, t);
-        const unsigned local = t - b.xstart[g], inst = local / b.xt[g], tile = local % b.xt[g];
-        const PassArgs<R>& a = b.args[g];
-        switch (b.lx[g]) {
-#define GPE_BATCH_XF(L)                                                                       \
-    case L:                                                                                   \
-        xpass_tile<R, L, 1, XK_FWD>(a, batch_rows(L), tile, inst, b.xt[g], smem_raw);          \
-        break;
-            GPE_BATCH_LENGTHS(GPE_BATCH_XF)
-#undef GPE_BATCH_XF
-            default:
-                break;
-        }
+        batch_tile_a(b, t, smem_raw);
         __syncthreads();  // the next tile reuses the exchange storage
     }
     if (!grid_sync_bounded(b.bar, b.wait_bound)) return;
-    // phase B: y forward * k-space * inverse
     for (unsigned t = blockIdx.x; t < b.sstart[ng]; t += gridDim.x) {
-        const int g = batch_group_of(b.sstart, ng, t);
-        const unsigned local = t - b.sstart[g], inst = local / b.st[g], tile = local % b.st[g];
-        const PassArgs<R>& a = b.args[BATCH_MAX_GROUPS + g];
-        switch (b.ly[g]) {
-#define GPE_BATCH_S(L)                                                                        \
-    case L:                                                                                   \
-        spass_tile<R, L, 1, batch_rows(L)>(a, b.ntx[g], tile, inst, smem_raw);                 \
-        break;
-            GPE_BATCH_LENGTHS(GPE_BATCH_S)
-#undef GPE_BATCH_S
-            default:
-                break;
-        }
+        batch_tile_b(b, t, smem_raw);
         __syncthreads();
     }
     if (!grid_sync_bounded(b.bar, b.wait_bound)) return;
-    // phase C: x inverse with the RK4 imaginary-time epilogue and reductions
     for (unsigned t = blockIdx.x; t < b.xstart[ng]; t += gridDim.x) {
-        const int g = batch_group_of(b.xstart, ng, t);
-        const unsigned local = t - b.xstart[g], inst = local / b.xt[g], tile = local % b.xt[g];
-        const PassArgs<R>& a = b.args[2 * BATCH_MAX_GROUPS + g];
-        switch (b.lx[g]) {
-#define GPE_BATCH_XI(L)                                                                       \
-    case L:                                                                                   \
-        xpass_tile<R, L, 1, XK_RKI>(a, batch_rows(L), tile, inst, b.xt[g], smem_raw);          \
-        break;
-            GPE_BATCH_LENGTHS(GPE_BATCH_XI)
-#undef GPE_BATCH_XI
-            default:
-                break;
-        }
+        batch_tile_c(b, t, smem_raw);
         __syncthreads();
     }
+}
+
+// One phase of one stage for every instance of every group, one tile per
+// CTA (grid = the phase's tile count): the grouped launch mode, three
+// launches a stage with programmatic dependent launch between them.  The
+// phase's own bodies only, so its registers are the phase's, not the whole
+// stage's.
+template <typename R, int PHASE>
+__host__ __device__ constexpr int batch_phase_min_blocks() {
+    return sizeof(R) == 4 ? (PHASE == 2 ? 2 : 3) : 2;
+}
+
+template <typename R, int PHASE>
+__global__ void __launch_bounds__(BATCH_THREADS, (batch_phase_min_blocks<R, PHASE>())) k_batch_phase(BatchStage<R> b) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    pass_prologue_sync();
+    if constexpr (PHASE == 0) batch_tile_a(b, blockIdx.x, smem_raw);
+    else if constexpr (PHASE == 1) batch_tile_b(b, blockIdx.x, smem_raw);
+    else batch_tile_c(b, blockIdx.x, smem_raw);
 }
 
 }  // namespace gpe

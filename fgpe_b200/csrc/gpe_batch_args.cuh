@@ -60,6 +60,10 @@ size_t batch_stage_smem(int esz);
 // CTAs per SM, SMs, cooperative launch support, dynamic shared memory.
 cudaError_t batch_stage_attributes(int esz, long long* out);
 bool batch_length_supported(int L);
+// One phase (0 = x forward, 1 = strided, 2 = x inverse) of stage b for every
+// instance, one tile per CTA, with programmatic dependent launch.
+cudaError_t launch_batch_phase(const BatchStage<float>& b, int phase, cudaStream_t st);
+cudaError_t launch_batch_phase(const BatchStage<double>& b, int phase, cudaStream_t st);
 cudaError_t launch_batch_stage(const BatchStage<float>& b, unsigned max_tiles, cudaStream_t st, BatchLaunchInfo* info);
 cudaError_t launch_batch_stage(const BatchStage<double>& b, unsigned max_tiles, cudaStream_t st,
                                BatchLaunchInfo* info);

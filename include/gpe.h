@@ -250,6 +250,30 @@ gpe_status gpe_dsz_dt(gpe_handle* h, double* out);
  * (CUFFT_INVERSE): the cufftExecZ2Z calls of src/baseHamiltonian.cu:89,95. */
 gpe_status gpe_fft(gpe_handle* h, int comp, int sign);
 
+/* ---- initial-state seeds on the device --------------------------------------
+ * Psi::imprintVortexTube (src/psi.cu:155-164) and the Psi::force*Lattice
+ * seeds (src/psi.cu:179-348) on component comp of the handle's psi, in FP64
+ * whatever the precision (a complex64 handle keeps the seeded complex128
+ * field as its compensated high + low parts).  The seeds add
+ * amp * shape(x - off) * (seed_npart / DV)^(1/2) to psi and renormalise it to
+ * norm_npart (Psi::add_lattice + Psi::normalize; the reference takes
+ * seed_npart from the seed's component and norm_npart from component 1).
+ * Grid points are cell centred: x_i = -xmax + i dx + dx/2. */
+enum gpe_lattice {
+    GPE_LATTICE_1D = 1,             /* amp (1 - cos k x) / 2            */
+    GPE_LATTICE_2D_TRIANGULAR = 2,  /* three cosines at 120 degrees     */
+    GPE_LATTICE_2D_SQUARE = 3,
+    GPE_LATTICE_3D_HEX = 4,
+    GPE_LATTICE_3D_FCC = 5,
+    GPE_LATTICE_3D_BCC = 6,
+    GPE_LATTICE_3D_SC = 7
+};
+/* psi *= exp(i Ncirc 2 pi x / (2 xmax_x)). */
+gpe_status gpe_imprint_vortex_tube(gpe_handle* h, int comp, double ncirc);
+/* off: 3 offsets (the unused ones of 1D/2D seeds are ignored). */
+gpe_status gpe_seed_lattice(gpe_handle* h, int comp, int lattice, double amp, double k, const double* off,
+                            double seed_npart, double norm_npart);
+
 /* ---- optimal-control gradient (no counterpart in the reference) ------------
  * Real-time RK4 (the gpe_step_real scheme, one component, GPE_HAM_BEC,
  * GPE_HAM_DIPOLAR or GPE_HAM_SOFT) where step n uses the potential
@@ -297,6 +321,18 @@ gpe_status gpe_batch_step_imag(gpe_batch* b, int nsteps, int* iters_done, int* c
 gpe_status gpe_batch_imag_state(gpe_batch* b, int inst, double* out);
 /* Kernels of this library run for the batch so far (graph replays included). */
 long long  gpe_batch_kernel_launches(const gpe_batch* b);
+/* Launch modes of a batch's imaginary-time iterations.
+ *   GPE_BATCH_PER_GROUP  one launch per pass per geometry group (12 per group
+ *                        an iteration), the tuned pass variants (default);
+ *   GPE_BATCH_PERSISTENT one cooperative launch per RK4 stage (4 an iteration,
+ *                        see gpe_batch_set_persistent);
+ *   GPE_BATCH_GROUPED    one launch per pass over the tiles of every group
+ *                        (12 an iteration), one tile per CTA.
+ * The two all-group modes share the conditions of gpe_batch_set_persistent;
+ * wait_bound applies to GPE_BATCH_PERSISTENT. */
+enum gpe_batch_mode { GPE_BATCH_PER_GROUP = 0, GPE_BATCH_PERSISTENT = 1, GPE_BATCH_GROUPED = 2 };
+gpe_status gpe_batch_set_launch_mode(gpe_batch* b, int mode, unsigned int wait_bound);
+int        gpe_batch_launch_mode(const gpe_batch* b);
 /* Persistent launches: one cooperative kernel per RK4 stage runs the stage's
  * three passes for every instance of every group, with a grid-wide barrier
  * between the passes (4 launches an iteration instead of 12 per group).

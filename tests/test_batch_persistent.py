@@ -19,7 +19,8 @@ import numpy as np
 import pytest
 
 import oracle_py as orc
-from fgpe_b200 import C64, C128, IMAG_RK4, Batch, GPEError, Solver, make_config
+from fgpe_b200 import (BATCH_GROUPED, BATCH_PER_GROUP, BATCH_PERSISTENT, C64, C128, IMAG_RK4, Batch, GPEError, Solver,
+                       make_config)
 
 from test_oracle import gaussian, harmonic
 
@@ -60,20 +61,24 @@ def fill(b, cfgs):
 SIZES = [64, 96, 64, 128, 192, 96, 256, 384, 512]
 
 
+@pytest.mark.parametrize("mode", [BATCH_PERSISTENT, BATCH_GROUPED])
 @pytest.mark.parametrize("prec", [C64, C128])
-def test_persistent_matches_per_group_and_oracle(gpu, prec):
+def test_persistent_matches_per_group_and_oracle(gpu, prec, mode):
+    """Both all-group modes (one cooperative launch per stage; one launch per
+    pass over every group's tiles) against the per-group launches and the
+    oracle."""
     cfgs = sweep_cfgs(prec, SIZES)
     nit = 5
     out = {}
-    for persistent in (False, True):
+    for m in (BATCH_PER_GROUP, mode):
         with Batch(cfgs) as b:
-            if persistent:
-                b.set_persistent(True)
-                assert b.persistent
+            if m != BATCH_PER_GROUP:
+                b.set_launch_mode(m)
+                assert b.launch_mode == m and b.persistent == (m == BATCH_PERSISTENT)
             fill(b, cfgs)
             it, cv = b.step_imag(nit)
-            out[persistent] = ([b.get_psi(i) for i in range(len(cfgs))],
-                               [b.imag_state(i) for i in range(len(cfgs))], it, cv)
+            out[m != BATCH_PER_GROUP] = ([b.get_psi(i) for i in range(len(cfgs))],
+                                         [b.imag_state(i) for i in range(len(cfgs))], it, cv)
     for i in range(len(cfgs)):
         assert rel(out[True][0][i], out[False][0][i]) < SAME_TOL[prec], i
         assert np.allclose(out[True][1][i], out[False][1][i], rtol=SAME_TOL[prec], atol=0), i
@@ -107,9 +112,16 @@ def test_persistent_launches_four_kernels_per_iteration(gpu):
         l1 = b.launches
         b.step_imag(3)
         per_stage = b.launches - l1
+        b.set_launch_mode(BATCH_GROUPED)
+        fill(b, cfgs)
+        b.step_imag(1)
+        l2 = b.launches
+        b.step_imag(3)
+        grouped = b.launches - l2
     # per call one iteration-counter reset per group; per iteration 4 stage
-    # kernels (per group: 3 passes x 4 stages)
+    # kernels, or 3 passes x 4 stages for all groups, or that per group
     assert per_stage == len(cfgs) + 4 * 3
+    assert grouped == len(cfgs) + 12 * 3
     assert per_group == len(cfgs) + 12 * 3 * len(cfgs)
 
 
