@@ -359,6 +359,14 @@ def run_ours(args):
     if not args.quick:
         line["accuracy"] = accuracy(solvers, psi_gs, args.accuracy_steps)
         line["cpu_baseline"] = cpu_baseline(n, psi_gs, solvers)
+        if world == 1:
+            # the reference's own CUDA build (complex128, cuFFT) on this GPU,
+            # same loop: the GPU-vs-GPU comparison figure
+            rb = reference_cuda_build(n)
+            if "steps_per_s" in rb:
+                rb["c64_over_reference_build"] = round(value / rb["steps_per_s"], 3)
+                rb["c128_over_reference_build"] = round(value128 / rb["steps_per_s"], 3)
+            line["reference_cuda_build"] = rb
     else:
         line["cpu_baseline"] = None
     for s2 in solvers.values():

@@ -97,7 +97,7 @@ def test_torch_function_and_driver(gpu):
     loss = control_loss(ut, s, target, 4)
     loss.backward()
     L, grad = s.control_gradient(u, target, 4)
-    assert float(loss) == L
+    assert float(loss.detach()) == L
     assert np.allclose(ut.grad.numpy(), grad, rtol=0, atol=0)
     _, losses = optimise(s, u, target, iters=4, lr=0.2, checkpoint_every=4)
     assert losses[-1] < losses[0]
