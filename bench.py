@@ -10,7 +10,8 @@ coefficients and FP64 compensated reductions; the plain complex128 drop-in is
 timed beside it, and the accuracy of the complex64 form after 10^4 steps is
 reported against complex128 (pinned to the FP64 oracle by the test suite).
 
-One "step" = one full RK4 step (4 stages x 5 fused axis passes).  L2 is
+One "step" = one full RK4 step (4 stages x 4 fused axis passes, run as one
+persistent launch when the tuner picks the persistent step).  L2 is
 flushed (256 MiB write) before every timed step; each step is bracketed by
 CUDA events on the library's stream.  `--impl reference` times the FP64 host
 oracle port of the reference's algorithm (the reference has no CPU path).
@@ -36,7 +37,8 @@ L_BOX = 10.0
 G0, G1 = 1000.0, 1100.0
 DT = 5e-4
 PI_REF = 3.141592653589793
-F_PER_STEP_KERNELS = {"x_fwd": 2.0, "x_inv": 7.75, "s_fwd": 2.0, "s_inv": 2.0, "s_fki": 2.0, "x_full": 0.0}
+F_PER_STEP_KERNELS = {"x_fwd": 2.0, "x_inv": 7.75, "s_fwd": 2.0, "s_inv": 2.0, "s_fki": 2.0, "x_full": 0.0,
+                      "flow": 55.0}
 # Algorithmic field transfers per launch of each pass kind in the 1-component
 # complex64 real-time RK4 step (F = one field): x-forward reads the stage
 # state and writes the work field (it runs only before the first stage of a
@@ -44,6 +46,8 @@ F_PER_STEP_KERNELS = {"x_fwd": 2.0, "x_inv": 7.75, "s_fwd": 2.0, "s_inv": 2.0, "
 # epilogue of stage 1/2/3/4 moves 5/7/7/8 fields (stage 4 also reads and
 # writes the low part of the compensated state) and writes the x-forward
 # transform of the state it produced for the next stage (+1 field): mean 7.75.
+# The persistent step kernel ("flow") runs all sixteen passes of a step in
+# one launch: 12 strided passes x 2 F + the four x passes' 6 + 8 + 8 + 9 F.
 
 
 def parse():
@@ -120,7 +124,7 @@ def cached_or_tune(cfg, workload, cache):
                     (cfg.nx, cfg.ny, cfg.nz, cfg.precision, nf, 1):
                 return {"default_us": d["default_us"], "tuned_us": d["tuned_us"], "from_cache": cache,
                         "variants": [d[k] for k in ("s10", "s11", "s12", "s20", "s21", "s22")],
-                        "xrows": d["xrows"], "yz": d.get("yz", 0)}
+                        "xrows": d["xrows"], "yz": d.get("yz", 0), "flow": d.get("flow", 0)}
     return gp.tune(cfg, workload, cache)
 
 
@@ -267,6 +271,21 @@ def run_ours(args):
             ms, launches, _ = time_steps(s, torch, flush, K, W)
             ms_p, _, prof = time_steps(s, torch, flush, K, W + K, profile=True)
             results[name] = {"ms": ms, "launches": launches, "ms_prof": ms_p, "prof": prof}
+        # the per-pass chain beside the persistent step (same handle, same work)
+        s = solvers["c64"]
+        persistent = {"active": s.flow_active}
+        if s.flow_active:
+            s.set_flow(False)
+            for w in range(W):
+                flush.zero_()
+                s.step_real(W + 2 * K + w, 1)
+            ms_chain, l_chain, _ = time_steps(s, torch, flush, K, 2 * W + 2 * K)
+            s.set_flow(True)
+            persistent.update({"ms_per_step_persistent": round(results["c64"]["ms"] / K, 5),
+                               "ms_per_step_chain": round(ms_chain / K, 5),
+                               "launches_per_step_persistent": results["c64"]["launches"] / K,
+                               "launches_per_step_chain": l_chain / K,
+                               "speedup_persistent_over_chain": round(ms_chain / results["c64"]["ms"], 3)})
     clocks = clk.summary()
 
     # max over ranks
@@ -350,6 +369,7 @@ def run_ours(args):
                      "per_kind_ms_per_launch": {k: round(v[0] / v[1], 5) for k, v in prof.items() if v[1]},
                      "profiled_ms_per_step": round(results["c64"]["ms_prof"] / K, 5)},
         "e2e": e2e,
+        "persistent_step": persistent,
         "tuning": tuning or "off (--no-tune): default pass variants",
         "gpu_launches": results["c64"]["launches"],
         "clocks": clocks,

@@ -36,7 +36,7 @@ BATCH_PER_GROUP, BATCH_PERSISTENT, BATCH_GROUPED = 0, 1, 2
 # gpe_lattice (include/gpe.h): Psi::force*Lattice seeds
 LATTICE_1D, LATTICE_2D_TRIANGULAR, LATTICE_2D_SQUARE, LATTICE_3D_HEX, LATTICE_3D_FCC, LATTICE_3D_BCC, \
     LATTICE_3D_SC = 1, 2, 3, 4, 5, 6, 7
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported", 3: "CUDA error",
           4: "out of memory", 5: "diverged", 6: "timeout", 7: "I/O error"}
@@ -137,6 +137,9 @@ def lib() -> ctypes.CDLL:
         "gpe_set_pass_variants": (c_int, [H, POINTER(c_int)]),
         "gpe_pass_variant_exists": (c_int, [POINTER(GPEConfig), c_int, c_int]),
         "gpe_set_user_hamiltonian": (c_int, [H, c_void_p]),
+        "gpe_set_flow": (c_int, [H, c_int, ctypes.c_uint]),
+        "gpe_flow_active": (c_int, [H]),
+        "gpe_flow_status": (c_int, [H, POINTER(c_int)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -211,10 +214,11 @@ def tune(cfg: GPEConfig, workload: int = 0, cache_path: str | None = None) -> di
     """Autotune the pass variants of cfg's grid (gpe_tune): workload 0 =
     real-time RK4 steps, 1 = imaginary-time iterations.  Stores the result
     in the JSON-lines cache_path when given."""
-    rep = np.zeros(11)
+    rep = np.zeros(12)
     _check(lib().gpe_tune(byref(cfg), workload, cache_path.encode() if cache_path else None, _dp(rep)))
     return {"default_us": float(rep[0]), "tuned_us": float(rep[1]), "timed": int(rep[2]),
-            "variants": [int(x) for x in rep[3:9]], "xrows": int(rep[9]), "yz": int(rep[10])}
+            "variants": [int(x) for x in rep[3:9]], "xrows": int(rep[9]), "yz": int(rep[10]),
+            "flow": int(rep[11])}
 
 
 def set_tune_cache(path: str | None) -> None:
@@ -407,7 +411,23 @@ class Solver:
     def launches(self) -> int:
         return int(lib().gpe_kernel_launches(self._h))
 
-    PROF_KINDS = ("x_fwd", "x_inv", "x_full", "s_fwd", "s_inv", "s_fki")
+    PROF_KINDS = ("x_fwd", "x_inv", "x_full", "s_fwd", "s_inv", "s_fki", "flow")
+
+    def set_flow(self, on: bool, wait_bound: int = 0) -> None:
+        """Real-time RK4 steps as one persistent launch per step (gpe_set_flow);
+        wait_bound 0 keeps the current bound."""
+        _check(lib().gpe_set_flow(self._h, 1 if on else 0, int(wait_bound)))
+
+    @property
+    def flow_active(self) -> bool:
+        return bool(lib().gpe_flow_active(self._h))
+
+    def flow_status(self) -> int:
+        """0, or GPE_ERR_TIMEOUT when a persistent step gave up since the last
+        call (the step's counters are then re-armed)."""
+        st = c_int(0)
+        _check(lib().gpe_flow_status(self._h, byref(st)))
+        return int(st.value)
 
     def set_user_hamiltonian(self, ops_ptr: int) -> None:
         """Install a user Hamiltonian plugin (the gpe_user_hamiltonian table a

@@ -12,6 +12,7 @@
 
 #include "../../include/gpe.h"
 #include "gpe_dispatch.cuh"
+#include "gpe_flow_args.cuh"
 #include "gpe_init.cuh"
 #include "gpe_sizes.h"
 
@@ -89,6 +90,13 @@ struct gpe_handle {
     // 1: the strided part of a 3D complex64 stage runs as the fused y-z
     // cluster kernel (k_yz, gpe_yz.cuh) where the grid allows it
     int yz = 0;
+    // 1: real-time RK4 steps of a complex64 one-component cubic grid run as
+    // one persistent launch per step (k_flow_step, gpe_flow.cuh); its
+    // dependency counters, the launch parity and the wait bound
+    int flow = 0;
+    FlowSync* flow_sync = nullptr;
+    long long flow_launches = 0;
+    unsigned flow_bound = 1u << 22;
     double* kax[3] = {nullptr, nullptr, nullptr};
     float* k2s[3] = {nullptr, nullptr, nullptr};  // complex64: lap_scale * k^2 per axis
     double* obs_part = nullptr;                    // OBS_BLOCKS partial sums + the result
@@ -688,6 +696,81 @@ gpe_status copy_field(gpe_handle* h, void* dst, const void* src) {
     return GPE_OK;
 }
 
+// Whether real-time steps of this handle run as one persistent launch per
+// step (k_flow_step, gpe_flow.cuh): complex64, one component and one
+// transformed field, a built-in pointwise Hamiltonian, a cubic grid the
+// kernel is compiled for, and the option on (gpe_set_flow or the tuner).
+bool flow_eligible(const gpe_handle* h) {
+    return h->prec == GPE_C64 && h->ncomp == 1 && h->nf == 1 && h->nb == 1 &&
+           (h->cfg.hamiltonian == GPE_HAM_BEC || h->cfg.hamiltonian == GPE_HAM_TEMPLATE) && h->nx % 2 == 0 &&
+           flow_shape_supported(h->nx, h->ny, h->nz);
+}
+bool flow_usable(const gpe_handle* h) { return h->flow && h->flow_sync && flow_eligible(h); }
+
+// Switches the persistent step on (allocating and zeroing its counters) or
+// off; bound = 0 keeps the current wait bound.
+gpe_status flow_enable(gpe_handle* h, int on, unsigned bound) {
+    if (bound) h->flow_bound = bound;
+    h->flow = on ? 1 : 0;
+    if (!on) return GPE_OK;
+    if (!h->flow_sync) GPE_CUDA(cudaMalloc((void**)&h->flow_sync, sizeof(FlowSync)));
+    GPE_CUDA(cudaMemsetAsync(h->flow_sync, 0, sizeof(FlowSync), h->st));
+    h->flow_launches = 0;
+    return GPE_OK;
+}
+
+// One real-time RK4 step as one launch: the strided passes take the
+// arguments launch_s would give them, the x tiles those of launch_x with the
+// fused stage epilogue (sa[s-1]: the arguments of stage s).
+template <typename R>
+gpe_status launch_flow_step(gpe_handle* h, const PassArgs<R> (&sa)[4], bool obs) {
+    if constexpr (sizeof(R) == 4) {
+        ProfScope ps(h, GPE_PROF_FLOW);
+        FlowArgs fa;
+        std::memset(&fa, 0, sizeof(fa));
+        const int modes[3] = {SM_FWD, SM_FKI, SM_INV};
+        for (int m = 0; m < 3; ++m) {
+            PassArgs<float> a = sa[0];
+            const int axis = m == 1 ? 2 : 1;
+            a.mode = modes[m];
+            a.sax = axis;
+            a.tx = spass_tx(axis == 1 ? h->ny : h->nz, (int)sizeof(float2));
+            a.tw = (const float2*)h->tw[axis];
+            a.tw2 = h->tw2[axis];
+            a.sstride = axis == 1 ? (long long)h->nx : (long long)h->nx * h->ny;
+            a.ostride = axis == 1 ? (long long)h->nx * h->ny : (long long)h->nx;
+            fa.s[m] = a;
+        }
+        for (int s = 0; s < 4; ++s) {
+            fa.x[s] = sa[s];
+            fa.x[s].mode = XM_INV;
+            fa.x[s].tw = (const float2*)h->tw[0];
+        }
+        fa.sync = h->flow_sync;
+        fa.set = (int)(h->flow_launches & 1);
+        fa.ntx = flow_ntx(h->nx);
+        fa.rows = flow_rows(h->nx);
+        fa.wait_bound = h->flow_bound;
+        int dev = 0, sms = 0;
+        GPE_CUDA(cudaGetDevice(&dev));
+        GPE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        const int per_sm = flow_ctas_per_sm(h->nx);
+        if (per_sm < 1) return fail(GPE_ERR_CUDA, "persistent step kernel: no resident CTA");
+        cudaError_t err = cudaSuccess;
+        if (!dispatch_flow(h->nx, obs, fa, sms * per_sm, h->st, &err))
+            return fail(GPE_ERR_UNSUPPORTED, "no persistent step kernel for this grid");
+        if (err != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("persistent step launch: ") + cudaGetErrorString(err));
+        h->flow_launches++;
+        h->launches++;
+        return GPE_OK;
+    } else {
+        (void)h;
+        (void)sa;
+        (void)obs;
+        return fail(GPE_ERR_UNSUPPORTED, "the persistent step kernel is complex64 only");
+    }
+}
+
 // ---- stepping ----------------------------------------------------------------------------
 // compensate: complex64 handles carry the step state as high (A) + low (Lo)
 // parts across steps and calls (rk_final_comp); off for the control
@@ -717,20 +800,37 @@ gpe_status step_real_t(gpe_handle* h, int first, int nsteps, double* obs_out, bo
     const bool can_fuse = h->ny > 1 || h->nz > 1;
     bool w_ready = can_fuse && h->w_fwd_A;
     h->w_fwd_A = false;
+    // the arguments of stage s of step `it` (the chain's and the persistent
+    // step kernel's alike)
+    auto stage_args = [&](PassArgs<R>& sa, int s, int it, bool want_obs) {
+        sa.stage = s;
+        for (int c = 0; c < 2; ++c) sa.pin[c] = (s == 1) ? (const C*)h->A[c] : (const C*)h->B[c];
+        // src/oneComponentGPSolver.cu:137-138,155,175,184: m05Idt, mIdt and PARS[T]
+        sa.c_re = 0.0;
+        sa.c_im = (s <= 2) ? -0.5 * dt : -1.0 * dt;
+        sa.t = (s == 1) ? (double)it * dt : (s < 4) ? (it + 0.5) * dt : (double)(it + 1) * dt;
+        sa.want_obs = (want_obs && s == 4) ? 1 : 0;
+        sa.fuse_fwd = (can_fuse && !sa.want_obs) ? 1 : 0;
+        // stages 1-3 use alg_calcHpsiMU, stage 4 alg_calcHpsi
+        // (src/oneComponentGPSolver.cu:170-190)
+        set_rotation<R>(h, sa, s == 4 && h->ncomp == 1);
+    };
+    const bool flow = flow_usable(h);
     for (int j = 0; j < nsteps; ++j) {
         const int it = first + j;
+        const bool obs_step = obs_out != nullptr && j == nsteps - 1;
+        if (flow) {
+            PassArgs<R> sa[4] = {a, a, a, a};
+            for (int s = 1; s <= 4; ++s) stage_args(sa[s - 1], s, it, obs_step);
+            if (sa[3].rot[0] == 0.0) {  // the moving-frame term runs on the chain
+                if (!w_ready) GPE_TRY(launch_x<R>(h, sa[0], h->nf, XM_FWD));
+                GPE_TRY(launch_flow_step<R>(h, sa, obs_step));
+                w_ready = !obs_step;
+                continue;
+            }
+        }
         for (int s = 1; s <= 4; ++s) {
-            a.stage = s;
-            for (int c = 0; c < 2; ++c) a.pin[c] = (s == 1) ? (const typename Cx<R>::T*)h->A[c] : (const typename Cx<R>::T*)h->B[c];
-            // src/oneComponentGPSolver.cu:137-138,155,175,184: m05Idt, mIdt and PARS[T]
-            a.c_re = 0.0;
-            a.c_im = (s <= 2) ? -0.5 * dt : -1.0 * dt;
-            a.t = (s == 1) ? (double)it * dt : (s < 4) ? (it + 0.5) * dt : (double)(it + 1) * dt;
-            a.want_obs = (obs_out != nullptr && j == nsteps - 1 && s == 4) ? 1 : 0;
-            a.fuse_fwd = (can_fuse && !a.want_obs) ? 1 : 0;
-            // stages 1-3 use alg_calcHpsiMU, stage 4 alg_calcHpsi
-            // (src/oneComponentGPSolver.cu:170-190)
-            set_rotation<R>(h, a, s == 4 && h->ncomp == 1);
+            stage_args(a, s, it, obs_step);
             GPE_TRY(run_chain<R>(h, a, h->nf, w_ready));
             w_ready = a.fuse_fwd != 0;
         }
@@ -975,7 +1075,7 @@ void free_all(gpe_handle* h) {
     for (void* p : ptrs)
         if (p) cudaFree(p);
     void* cptrs[] = {h->ctrlG, h->V0, h->adj[0], h->adj[1], h->adj[2], h->adj[3], h->adj[4], h->adj[5], h->adj[6],
-                     h->qf, h->d_u, h->d_part, h->d_grad};
+                     h->qf, h->d_u, h->d_part, h->d_grad, h->flow_sync};
     for (void* p : cptrs)
         if (p) cudaFree(p);
     for (void* p : h->cps)
@@ -2360,7 +2460,7 @@ std::string tune_line(const gpe_handle* h, double def_us, double tuned_us) {
       << ",\"nf\":" << k.nf << ",\"nb\":" << k.nb;
     for (int ax = 1; ax <= 2; ++ax)
         for (int m = 0; m < 3; ++m) o << ",\"s" << ax << m << "\":" << h->svar[ax][m];
-    o << ",\"xrows\":" << h->xrows << ",\"yz\":" << h->yz;
+    o << ",\"xrows\":" << h->xrows << ",\"yz\":" << h->yz << ",\"flow\":" << h->flow;
     char buf[64];
     std::snprintf(buf, sizeof(buf), ",\"default_us\":%.3f,\"tuned_us\":%.3f}", def_us, tuned_us);
     o << buf;
@@ -2391,6 +2491,8 @@ void tune_apply_cache(gpe_handle* h) {
     if (json_int(hit, "xrows", &r) && r >= 0 && r <= 256) h->xrows = r;
     int yz = 0;
     if (json_int(hit, "yz", &yz) && (yz == 0 || (yz == 1 && yz_usable(h, h->nf)))) h->yz = yz;
+    int fl = 0;
+    if (json_int(hit, "flow", &fl) && fl == 1 && flow_eligible(h)) flow_enable(h, 1, 0);
 }
 
 // Replaces the line of h's key in the cache file (or appends it).
@@ -2561,6 +2663,25 @@ gpe_status tune_handle_t(gpe_handle* h, int workload, double* report) {
     }
     double tuned_us = 0.0;
     GPE_TRY(time_steps<R>(h, workload, &tuned_us));
+    // real-time steps as one persistent launch each (same arithmetic)
+    if (workload == 0 && flow_eligible(h)) {
+        double us = 0.0;
+        gpe_status s = flow_enable(h, 1, 0);
+        if (s == GPE_OK) s = time_steps<R>(h, workload, &us);
+        ++timed;
+        int st = 0;
+        if (h->flow_sync) {
+            cudaStreamSynchronize(h->st);
+            cudaMemcpy(&st, &h->flow_sync->status, sizeof(int), cudaMemcpyDeviceToHost);
+        }
+        if (s != GPE_OK || st != 0 || !(us < tuned_us * 0.99)) {
+            cudaGetLastError();
+            h->flow = 0;
+        } else {
+            tuned_us = us;
+        }
+        GPE_CUDA(cudaStreamSynchronize(h->st));
+    }
     if (report) {
         report[0] = def_us;
         report[1] = tuned_us;
@@ -2580,6 +2701,7 @@ gpe_status tune_config(const gpe_config* cfg, int nb, int workload, double* repo
         for (int m = 0; m < 3; ++m) h->svar[ax][m] = 0;
     h->xrows = 0;
     h->yz = 0;
+    h->flow = 0;
     gpe_status s = h->prec == GPE_C64 ? tune_handle_t<float>(h, workload, report)
                                       : tune_handle_t<double>(h, workload, report);
     if (s != GPE_OK) {
@@ -2618,11 +2740,41 @@ gpe_status gpe_tune(const gpe_config* cfg, int workload, const char* cache_path,
             for (int m = 0; m < 3; ++m) report[3 + (ax - 1) * 3 + m] = h->svar[ax][m];
         report[9] = h->xrows;
         report[10] = h->yz;
+        report[11] = h->flow;
     }
     cudaStreamSynchronize(h->st);
     free_all(h);
     delete h;
     return s;
+}
+
+gpe_status gpe_set_flow(gpe_handle* h, int on, unsigned wait_bound) {
+    GPE_TRY(check_handle(h));
+    if (on != 0 && on != 1) return fail(GPE_ERR_INVALID_ARG, "on must be 0 or 1");
+    GPE_TRY(flow_enable(h, on, wait_bound));
+    GPE_CUDA(cudaStreamSynchronize(h->st));
+    return GPE_OK;
+}
+
+int gpe_flow_active(const gpe_handle* h) { return h && flow_usable(h) ? 1 : 0; }
+
+gpe_status gpe_flow_status(gpe_handle* h, int* status_out) {
+    GPE_TRY(check_handle(h));
+    if (!status_out) return fail(GPE_ERR_INVALID_ARG, "null status");
+    *status_out = 0;
+    GPE_CUDA(cudaStreamSynchronize(h->st));
+    if (!h->flow_sync) return GPE_OK;
+    int st = 0;
+    GPE_CUDA(cudaMemcpy(&st, &h->flow_sync->status, sizeof(int), cudaMemcpyDeviceToHost));
+    *status_out = st;
+    if (st != 0) {  // re-arm: counters, tickets and both status words
+        GPE_CUDA(cudaMemset(h->flow_sync, 0, sizeof(FlowSync)));
+        int hs = 0;
+        GPE_CUDA(cudaMemcpy(&hs, &h->sc->status, sizeof(int), cudaMemcpyDeviceToHost));
+        if (hs == GPE_ERR_TIMEOUT) GPE_CUDA(cudaMemset(&h->sc->status, 0, sizeof(int)));
+        h->flow_launches = 0;
+    }
+    return GPE_OK;
 }
 
 gpe_status gpe_get_pass_variants(const gpe_handle* h, int* out) {

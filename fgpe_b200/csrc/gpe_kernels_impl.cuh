@@ -1036,20 +1036,23 @@ __device__ __forceinline__ void spec_point2(const PassArgs<float>& a, cpair (&v)
     }
 }
 
-template <int L, int NF, int TXP, int MB, int PV>
-__global__ void __launch_bounds__(TXP * Plan<L, PV>::T, MB) k_spass2(PassArgs<float> a, int ntx) {
+// One tile of a paired strided pass (tile = outer * ntx + x block) of
+// instance inst, after the wait on the previous grid; k_spass2 runs one tile
+// per CTA, the persistent RK4 step kernel (gpe_flow.cuh) runs many.
+template <int L, int NF, int TXP, int PV>
+__device__ __forceinline__ void spass2_tile(const PassArgs<float>& a, int ntx, unsigned tile, unsigned inst,
+                                            unsigned char* smem_raw) {
     typedef Plan<L, PV> PL;
     constexpr int E = PL::E;
     constexpr int T = PL::T;
     constexpr int RinF = PL::in_radix(false);
     constexpr int RoutF = PL::out_radix(false);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    pass_prologue_sync();
-    const long long boff = select_instance(a).boff;
-    if (a.check_done && (a.sc + (a.nbatch > 1 ? blockIdx.y : 0))->done) return;
+    const InstPtr ip = select_instance_at(a, inst);
+    const long long boff = ip.boff;
+    if (a.check_done && ip.sc->done) return;
 
     cpair* X = reinterpret_cast<cpair*>(smem_raw);
-    const int xb = blockIdx.x % ntx, outer = blockIdx.x / ntx;
+    const int xb = (int)tile % ntx, outer = (int)tile / ntx;
     const int x0 = xb * (2 * TXP);
     const unsigned b = threadIdx.x % TXP, t = threadIdx.x / TXP;
     const int xa = x0 + 2 * (int)b;
@@ -1121,6 +1124,13 @@ __global__ void __launch_bounds__(TXP * Plan<L, PV>::T, MB) k_spass2(PassArgs<fl
             for (int f = 0; f < NF; ++f) *reinterpret_cast<float4*>(a.w[f] + gi) = pair_to(v[f][e]);
         }
     }
+}
+
+template <int L, int NF, int TXP, int MB, int PV>
+__global__ void __launch_bounds__(TXP * Plan<L, PV>::T, MB) k_spass2(PassArgs<float> a, int ntx) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    pass_prologue_sync();
+    spass2_tile<L, NF, TXP, PV>(a, ntx, blockIdx.x, a.nbatch > 1 ? blockIdx.y : 0u, smem_raw);
 }
 
 // ---- launchers ----------------------------------------------------------------------

@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define GPE_ABI_VERSION 1
+#define GPE_ABI_VERSION 2
 /* hpp/header.hpp:23  NO_HAMIL_PARAMS: size of d_h_params */
 #define GPE_NO_HAMIL_PARAMS 32
 
@@ -409,10 +409,11 @@ gpe_status gpe_norm_noalloc(const void* dev_psi_c128, long long n, double dv, do
  * workload, 0 = real-time RK4 steps, 1 = imaginary-time iterations), keeps
  * the fastest, and stores one line keyed by (nx, ny, nz, precision, fields,
  * instances = 1) in the JSON-lines file cache_path (replacing a line of the
- * same key; NULL = do not store).  report (may be NULL) receives 11 values:
+ * same key; NULL = do not store).  report (may be NULL) receives 12 values:
  * default and tuned microseconds per step, variants timed, the chosen
- * variants s[axis 1][mode 0..2], s[axis 2][mode 0..2], the rows and the
- * fused y-z flag. */
+ * variants s[axis 1][mode 0..2], s[axis 2][mode 0..2], the rows, the
+ * fused y-z flag and the persistent-step flag (gpe_set_flow; real-time
+ * workload only). */
 gpe_status gpe_tune(const gpe_config* cfg, int workload, const char* cache_path, double* report);
 /* Process-wide: gpe_create and gpe_batch_create apply the cache line that
  * matches a new handle (or batch group); NULL = read $GPE_TUNE_CACHE if set. */
@@ -432,6 +433,32 @@ gpe_status gpe_set_pass_variants(gpe_handle* h, const int* in8);
  * cfg's grid, precision and fields; variant 0 always does.  Host only. */
 int        gpe_pass_variant_exists(const gpe_config* cfg, int axis, int v);
 
+/* ---- persistent RK4 step (no counterpart in the reference, whose step is
+ * eight cuFFT calls and a dozen element-wise kernels,
+ * src/oneComponentGPSolver.cu:166-190) -------------------------------------
+ * on = 1: each real-time RK4 step of gpe_step_real runs as ONE launch whose
+ * CTAs take the tiles of the step's sixteen axis passes from one ordered list,
+ * every tile waiting only for the tiles whose output it reads (per x block
+ * or z plane), so the passes overlap instead of draining between launches.
+ * The tiles are the pass kernels' own, so the results equal the per-pass
+ * chain's bit for bit.  It serves complex64 one-component handles on cubic
+ * grids of length 128 or 256 with GPE_HAM_BEC or GPE_HAM_TEMPLATE and no
+ * moving-frame term; for every other handle, and for the step of a call that
+ * returns the logging observables, the per-pass chain runs (the option is
+ * kept).  wait_bound: 32 ns sleeps a tile's wait may take before the launch
+ * gives up (0 keeps the current bound, default 2^22); a launch that gives
+ * up records GPE_ERR_TIMEOUT in the handle's status word (reported by the
+ * next call that reads the device scalars, e.g. gpe_step_real with
+ * observables) and in the step's own status word, after which later
+ * persistent steps do nothing until gpe_flow_status re-arms them. */
+gpe_status gpe_set_flow(gpe_handle* h, int on, unsigned wait_bound);
+/* 1 when the handle's real-time steps run as the persistent step. */
+int        gpe_flow_active(const gpe_handle* h);
+/* Synchronises; *status_out = 0 or GPE_ERR_TIMEOUT (a persistent step gave
+ * up since the last call).  After a timeout the counters and both status
+ * words are reset; the fields hold the partial step and must be set again. */
+gpe_status gpe_flow_status(gpe_handle* h, int* status_out);
+
 /* Synchronise the handle's stream and report any asynchronous error. */
 gpe_status gpe_sync(gpe_handle* h);
 /* Number of this library's kernels launched by the handle so far. */
@@ -439,10 +466,12 @@ long long  gpe_kernel_launches(const gpe_handle* h);
 
 /* ---- measurement (no counterpart in the reference, whose only timing is
  * unsynchronised host chrono, src/oneComponentGPSolver.cu:153,197-200) ----- */
-#define GPE_PROF_KINDS 6
+#define GPE_PROF_KINDS 7
+#define GPE_PROF_FLOW 6
 /* Pass kinds: 0 x-forward (+prologue), 1 x-inverse (+epilogue), 2 x-full,
  * 3 strided forward, 4 strided inverse, 5 strided forward*k-space*inverse
- * (with the fused y-z kernel: that kernel, and no kinds 3 and 4). */
+ * (with the fused y-z kernel: that kernel, and no kinds 3 and 4), 6 the
+ * persistent RK4 step (gpe_set_flow: one launch for the whole step). */
 /* When enabled, every pass launch is bracketed by CUDA events on the
  * handle's stream. */
 gpe_status gpe_profile_enable(gpe_handle* h, int enable);

@@ -44,10 +44,10 @@ def test_every_declared_symbol_is_exported():
 def test_host_only_entry_points_work_without_gpu():
     import fgpe_b200 as g
     L = g.lib()
-    assert L.gpe_abi_version() == 1
+    assert L.gpe_abi_version() == 2
     cfg = g.GPEConfig()
     assert L.gpe_config_init(ctypes.byref(cfg)) == 0
-    assert cfg.abi_version == 1 and cfg.ncomp == 1 and cfg.nx == 1
+    assert cfg.abi_version == 2 and cfg.ncomp == 1 and cfg.nx == 1
     for n in (1, 2, 3, 5, 8, 96, 128, 192, 384, 512, 768, 1024, 25, 27, 864):
         assert L.gpe_fft_length_supported(n) == 1, n
     for n in (0, 7, 14, 2048, 15, 1536):

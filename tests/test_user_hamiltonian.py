@@ -30,7 +30,7 @@ def test_plugin_library_exports_its_table():
     L, ops = plugin_ops()
     assert ops
     tab = ctypes.cast(ops, ctypes.POINTER(ctypes.c_int))
-    assert tab[0] == 1  # GPE_ABI_VERSION
+    assert tab[0] == 2  # GPE_ABI_VERSION
     ptrs = ctypes.cast(ops + 8, ctypes.POINTER(ctypes.c_void_p))
     assert ptrs[0] and ptrs[1]
 
