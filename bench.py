@@ -70,6 +70,9 @@ def parse():
     p.add_argument("--no-tune", action="store_true", help="keep the default pass variants (no autotuning)")
     p.add_argument("--tune-cache", default=None,
                    help="JSON-lines tuning cache to reuse: grids with a line there are not tuned again")
+    p.add_argument("--persistent-step", default="tuned", choices=["tuned", "on", "off"],
+                   help="complex64 real-time steps as one persistent launch each (gpe_set_flow): the tuner's "
+                        "choice, forced on, or forced off")
     p.add_argument("--sweep-converge", action="store_true",
                    help="sweep2d: also run every instance to |dmu| < 1e-8 and report the iterations")
     return p.parse_args()
@@ -259,6 +262,8 @@ def run_ours(args):
         s.set_stream(stream_ptr)
         s.set_vext(0, trap(cfg))
         s.set_psi(0, psi_gs)
+        if name == "c64" and args.persistent_step != "tuned":
+            s.set_flow(args.persistent_step == "on")
         solvers[name] = s
 
     results = {}
