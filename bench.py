@@ -38,7 +38,7 @@ G0, G1 = 1000.0, 1100.0
 DT = 5e-4
 PI_REF = 3.141592653589793
 F_PER_STEP_KERNELS = {"x_fwd": 2.0, "x_inv": 7.75, "s_fwd": 2.0, "s_inv": 2.0, "s_fki": 2.0, "x_full": 0.0,
-                      "flow": 55.0}
+                      "flow": 55.0, "s_flow": 6.0}
 # Algorithmic field transfers per launch of each pass kind in the 1-component
 # complex64 real-time RK4 step (F = one field): x-forward reads the stage
 # state and writes the work field (it runs only before the first stage of a
@@ -47,7 +47,8 @@ F_PER_STEP_KERNELS = {"x_fwd": 2.0, "x_inv": 7.75, "s_fwd": 2.0, "s_inv": 2.0, "
 # writes the low part of the compensated state) and writes the x-forward
 # transform of the state it produced for the next stage (+1 field): mean 7.75.
 # The persistent step kernel ("flow") runs all sixteen passes of a step in
-# one launch: 12 strided passes x 2 F + the four x passes' 6 + 8 + 8 + 9 F.
+# one launch: 12 strided passes x 2 F + the four x passes' 6 + 8 + 8 + 9 F;
+# the persistent strided stage ("s_flow") the three strided passes of a stage.
 
 
 def parse():
@@ -70,9 +71,9 @@ def parse():
     p.add_argument("--no-tune", action="store_true", help="keep the default pass variants (no autotuning)")
     p.add_argument("--tune-cache", default=None,
                    help="JSON-lines tuning cache to reuse: grids with a line there are not tuned again")
-    p.add_argument("--persistent-step", default="tuned", choices=["tuned", "on", "off"],
-                   help="complex64 real-time steps as one persistent launch each (gpe_set_flow): the tuner's "
-                        "choice, forced on, or forced off")
+    p.add_argument("--persistent-step", default="tuned", choices=["tuned", "on", "strided", "off"],
+                   help="complex64 persistent launches (gpe_set_flow): the tuner's choice, one launch per step "
+                        "(on), one launch per stage's strided passes (strided), or the per-pass chain (off)")
     p.add_argument("--sweep-converge", action="store_true",
                    help="sweep2d: also run every instance to |dmu| < 1e-8 and report the iterations")
     return p.parse_args()
@@ -263,7 +264,7 @@ def run_ours(args):
         s.set_vext(0, trap(cfg))
         s.set_psi(0, psi_gs)
         if name == "c64" and args.persistent_step != "tuned":
-            s.set_flow(args.persistent_step == "on")
+            s.set_flow({"on": 1, "strided": 2, "off": 0}[args.persistent_step])
         solvers[name] = s
 
     results = {}
@@ -280,12 +281,13 @@ def run_ours(args):
         s = solvers["c64"]
         persistent = {"active": s.flow_active}
         if s.flow_active:
-            s.set_flow(False)
+            mode = s.flow_active
+            s.set_flow(0)
             for w in range(W):
                 flush.zero_()
                 s.step_real(W + 2 * K + w, 1)
             ms_chain, l_chain, _ = time_steps(s, torch, flush, K, 2 * W + 2 * K)
-            s.set_flow(True)
+            s.set_flow(mode)
             persistent.update({"ms_per_step_persistent": round(results["c64"]["ms"] / K, 5),
                                "ms_per_step_chain": round(ms_chain / K, 5),
                                "launches_per_step_persistent": results["c64"]["launches"] / K,

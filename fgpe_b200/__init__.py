@@ -411,16 +411,19 @@ class Solver:
     def launches(self) -> int:
         return int(lib().gpe_kernel_launches(self._h))
 
-    PROF_KINDS = ("x_fwd", "x_inv", "x_full", "s_fwd", "s_inv", "s_fki", "flow")
+    PROF_KINDS = ("x_fwd", "x_inv", "x_full", "s_fwd", "s_inv", "s_fki", "flow", "s_flow")
 
-    def set_flow(self, on: bool, wait_bound: int = 0) -> None:
-        """Real-time RK4 steps as one persistent launch per step (gpe_set_flow);
-        wait_bound 0 keeps the current bound."""
-        _check(lib().gpe_set_flow(self._h, 1 if on else 0, int(wait_bound)))
+    def set_flow(self, mode, wait_bound: int = 0) -> None:
+        """Persistent launches (gpe_set_flow): True / 1 = one launch per
+        real-time RK4 step, 2 = the three strided passes of each stage in
+        one launch, False / 0 = the per-pass chain; wait_bound 0 keeps the
+        current bound."""
+        _check(lib().gpe_set_flow(self._h, int(mode), int(wait_bound)))
 
     @property
-    def flow_active(self) -> bool:
-        return bool(lib().gpe_flow_active(self._h))
+    def flow_active(self) -> int:
+        """1 (whole step), 2 (strided stages) or 0 (per-pass chain)."""
+        return int(lib().gpe_flow_active(self._h))
 
     def flow_status(self) -> int:
         """0, or GPE_ERR_TIMEOUT when a persistent step gave up since the last

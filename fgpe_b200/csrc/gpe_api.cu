@@ -159,6 +159,19 @@ __global__ void k_lo_residual(float2* lo, const float2* hi, const double2* src, 
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i < n) lo[i] = make_float2((float)(src[i].x - (double)hi[i].x), (float)(src[i].y - (double)hi[i].y));
 }
+// A complex128 state into a complex64 handle in one pass: the high part
+// (rounded) into both state slots, the rounding residual into the low part
+// (k_from_c128, the copy of A into B and k_lo_residual, fused).
+__global__ void k_set_state_c64(float2* a, float2* b, float2* lo, const double2* src, long long n) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) {
+        const double2 v = src[i];
+        const float2 hi = make_float2((float)v.x, (float)v.y);
+        a[i] = hi;
+        b[i] = hi;
+        lo[i] = make_float2((float)(v.x - (double)hi.x), (float)(v.y - (double)hi.y));
+    }
+}
 // high + low parts of a compensated complex64 state
 __global__ void k_to_c128_hilo(double2* dst, const float2* hi, const float2* lo, long long n) {
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -628,6 +641,9 @@ gpe_status launch_yz_chain(gpe_handle* h, PassArgs<R> a) {
     }
 }
 
+bool flow_strided_usable(const gpe_handle* h, int nf);
+gpe_status launch_flow_strided(gpe_handle* h, const PassArgs<float>& a);
+
 template <typename R>
 gpe_status run_chain(gpe_handle* h, const PassArgs<R>& a, int nf, bool skip_fwd = false) {
     int axes[2], na = 0;
@@ -638,6 +654,12 @@ gpe_status run_chain(gpe_handle* h, const PassArgs<R>& a, int nf, bool skip_fwd 
     if (h->yz && yz_usable(h, nf)) {
         GPE_TRY(launch_yz_chain<R>(h, a));
         return launch_x<R>(h, a, nf, XM_INV);
+    }
+    if constexpr (sizeof(R) == 4) {
+        if (na == 2 && flow_strided_usable(h, nf)) {
+            GPE_TRY(launch_flow_strided(h, a));
+            return launch_x<R>(h, a, nf, XM_INV);
+        }
     }
     for (int i = 0; i < na - 1; ++i) GPE_TRY(launch_s<R>(h, a, nf, axes[i], SM_FWD));
     GPE_TRY(launch_s<R>(h, a, nf, axes[na - 1], SM_FKI));
@@ -705,17 +727,66 @@ bool flow_eligible(const gpe_handle* h) {
            (h->cfg.hamiltonian == GPE_HAM_BEC || h->cfg.hamiltonian == GPE_HAM_TEMPLATE) && h->nx % 2 == 0 &&
            flow_shape_supported(h->nx, h->ny, h->nz);
 }
-bool flow_usable(const gpe_handle* h) { return h->flow && h->flow_sync && flow_eligible(h); }
+bool flow_usable(const gpe_handle* h) { return h->flow == 1 && h->flow_sync && flow_eligible(h); }
+// Mode 2: the strided passes of a one-field complex64 chain on a cubic grid
+// the kernel is compiled for (any epilogue: the x passes keep their launches).
+bool flow_strided_usable(const gpe_handle* h, int nf) {
+    return h->flow == 2 && h->flow_sync && h->prec == GPE_C64 && nf == 1 && h->nb == 1 && h->nx % 2 == 0 &&
+           flow_shape_supported(h->nx, h->ny, h->nz);
+}
 
 // Switches the persistent step on (allocating and zeroing its counters) or
 // off; bound = 0 keeps the current wait bound.
 gpe_status flow_enable(gpe_handle* h, int on, unsigned bound) {
     if (bound) h->flow_bound = bound;
-    h->flow = on ? 1 : 0;
+    h->flow = on;
     if (!on) return GPE_OK;
     if (!h->flow_sync) GPE_CUDA(cudaMalloc((void**)&h->flow_sync, sizeof(FlowSync)));
     GPE_CUDA(cudaMemsetAsync(h->flow_sync, 0, sizeof(FlowSync), h->st));
     h->flow_launches = 0;
+    return GPE_OK;
+}
+
+// The arguments launch_s would give the y forward, z forward * k-space *
+// inverse and y inverse passes of a chain with arguments a.
+void flow_strided_args(const gpe_handle* h, const PassArgs<float>& a0, FlowArgs& fa) {
+    const int modes[3] = {SM_FWD, SM_FKI, SM_INV};
+    for (int m = 0; m < 3; ++m) {
+        PassArgs<float> a = a0;
+        const int axis = m == 1 ? 2 : 1;
+        a.mode = modes[m];
+        a.sax = axis;
+        a.tx = spass_tx(axis == 1 ? h->ny : h->nz, (int)sizeof(float2));
+        a.tw = (const float2*)h->tw[axis];
+        a.tw2 = h->tw2[axis];
+        a.sstride = axis == 1 ? (long long)h->nx : (long long)h->nx * h->ny;
+        a.ostride = axis == 1 ? (long long)h->nx * h->ny : (long long)h->nx;
+        fa.s[m] = a;
+    }
+}
+
+// The three strided passes of a one-field complex64 chain as one launch.
+gpe_status launch_flow_strided(gpe_handle* h, const PassArgs<float>& a) {
+    ProfScope ps(h, GPE_PROF_SFLOW);
+    FlowArgs fa;
+    std::memset(&fa, 0, sizeof(fa));
+    flow_strided_args(h, a, fa);
+    fa.sync = h->flow_sync;
+    fa.set = (int)(h->flow_launches & 1);
+    fa.ntx = flow_ntx(h->nx);
+    fa.wait_bound = h->flow_bound;
+    int dev = 0, sms = 0;
+    GPE_CUDA(cudaGetDevice(&dev));
+    GPE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int per_sm = flow_strided_ctas_per_sm(h->nx);
+    if (per_sm < 1) return fail(GPE_ERR_CUDA, "persistent strided stage: no resident CTA");
+    cudaError_t err = cudaSuccess;
+    if (!dispatch_flow_strided(h->nx, fa, sms * per_sm, h->st, &err))
+        return fail(GPE_ERR_UNSUPPORTED, "no persistent strided-stage kernel for this grid");
+    if (err != cudaSuccess)
+        return fail(GPE_ERR_CUDA, std::string("persistent strided-stage launch: ") + cudaGetErrorString(err));
+    h->flow_launches++;
+    h->launches++;
     return GPE_OK;
 }
 
@@ -728,19 +799,7 @@ gpe_status launch_flow_step(gpe_handle* h, const PassArgs<R> (&sa)[4], bool obs)
         ProfScope ps(h, GPE_PROF_FLOW);
         FlowArgs fa;
         std::memset(&fa, 0, sizeof(fa));
-        const int modes[3] = {SM_FWD, SM_FKI, SM_INV};
-        for (int m = 0; m < 3; ++m) {
-            PassArgs<float> a = sa[0];
-            const int axis = m == 1 ? 2 : 1;
-            a.mode = modes[m];
-            a.sax = axis;
-            a.tx = spass_tx(axis == 1 ? h->ny : h->nz, (int)sizeof(float2));
-            a.tw = (const float2*)h->tw[axis];
-            a.tw2 = h->tw2[axis];
-            a.sstride = axis == 1 ? (long long)h->nx : (long long)h->nx * h->ny;
-            a.ostride = axis == 1 ? (long long)h->nx * h->ny : (long long)h->nx;
-            fa.s[m] = a;
-        }
+        flow_strided_args(h, sa[0], fa);
         for (int s = 0; s < 4; ++s) {
             fa.x[s] = sa[s];
             fa.x[s].mode = XM_INV;
@@ -1536,12 +1595,33 @@ gpe_status gpe_set_params(gpe_handle* h, const double prms[GPE_NO_HAMIL_PARAMS])
     return GPE_OK;
 }
 
+// complex64 handles with a low part: the state of component comp from the
+// complex128 array src (device) in one kernel, no synchronisation.
+gpe_status set_state_c64(gpe_handle* h, int comp, const void* src) {
+    if (!h->lo_valid)
+        for (int c = 0; c < h->ncomp; ++c)
+            if (c != comp) GPE_CUDA(cudaMemsetAsync(h->Lo[c], 0, h->esz * h->N, h->st));
+    k_set_state_c64<<<blocks_for(h->N, 256), 256, 0, h->st>>>((float2*)h->A[comp], (float2*)h->B[comp],
+                                                               (float2*)h->Lo[comp], (const double2*)src, h->N);
+    h->launches++;
+    GPE_CUDA(cudaGetLastError());
+    h->lo_valid = true;
+    h->hb_old_valid = true;
+    return GPE_OK;
+}
+
 gpe_status gpe_set_psi(gpe_handle* h, int comp, const double* host_c128) {
     if (h) h->w_fwd_A = false;
     GPE_TRY(check_handle(h));
     GPE_TRY(check_comp(h, comp));
     if (!host_c128) return fail(GPE_ERR_INVALID_ARG, "null psi");
     GPE_TRY(canonicalize(h));
+    if (h->prec == GPE_C64 && h->Lo[comp]) {  // one copy, one kernel, one synchronisation
+        GPE_CUDA(cudaMemcpyAsync(h->stage128, host_c128, 16 * h->N, cudaMemcpyHostToDevice, h->st));
+        GPE_TRY(set_state_c64(h, comp, h->stage128));
+        GPE_CUDA(cudaStreamSynchronize(h->st));
+        return GPE_OK;
+    }
     GPE_TRY(upload_c128_host(h, host_c128, h->A[comp]));
     GPE_TRY(set_low_part(h, comp, h->stage128));
     GPE_CUDA(cudaMemcpyAsync(h->B[comp], h->A[comp], h->esz * h->N, cudaMemcpyDeviceToDevice, h->st));
@@ -1556,6 +1636,7 @@ gpe_status gpe_set_psi_device(gpe_handle* h, int comp, const void* dev_c128) {
     GPE_TRY(check_comp(h, comp));
     if (!dev_c128) return fail(GPE_ERR_INVALID_ARG, "null psi");
     GPE_TRY(canonicalize(h));
+    if (h->prec == GPE_C64 && h->Lo[comp]) return set_state_c64(h, comp, dev_c128);
     GPE_TRY(upload_c128_device(h, comp, dev_c128, h->A[comp]));
     GPE_TRY(set_low_part(h, comp, dev_c128));
     GPE_CUDA(cudaMemcpyAsync(h->B[comp], h->A[comp], h->esz * h->N, cudaMemcpyDeviceToDevice, h->st));
@@ -2492,7 +2573,7 @@ void tune_apply_cache(gpe_handle* h) {
     int yz = 0;
     if (json_int(hit, "yz", &yz) && (yz == 0 || (yz == 1 && yz_usable(h, h->nf)))) h->yz = yz;
     int fl = 0;
-    if (json_int(hit, "flow", &fl) && fl == 1 && flow_eligible(h)) flow_enable(h, 1, 0);
+    if (json_int(hit, "flow", &fl) && ((fl == 1 && flow_eligible(h)) || fl == 2)) flow_enable(h, fl, 0);
 }
 
 // Replaces the line of h's key in the cache file (or appends it).
@@ -2682,6 +2763,26 @@ gpe_status tune_handle_t(gpe_handle* h, int workload, double* report) {
         }
         GPE_CUDA(cudaStreamSynchronize(h->st));
     }
+    // the three strided passes of each stage as one persistent launch
+    if (h->flow == 0 && h->prec == GPE_C64 && h->nf == 1 && h->nb == 1 && h->nx % 2 == 0 &&
+        flow_shape_supported(h->nx, h->ny, h->nz)) {
+        double us = 0.0;
+        gpe_status s = flow_enable(h, 2, 0);
+        if (s == GPE_OK) s = time_steps<R>(h, workload, &us);
+        ++timed;
+        int st = 0;
+        if (h->flow_sync) {
+            cudaStreamSynchronize(h->st);
+            cudaMemcpy(&st, &h->flow_sync->status, sizeof(int), cudaMemcpyDeviceToHost);
+        }
+        if (s != GPE_OK || st != 0 || !(us < tuned_us * 0.99)) {
+            cudaGetLastError();
+            h->flow = 0;
+        } else {
+            tuned_us = us;
+        }
+        GPE_CUDA(cudaStreamSynchronize(h->st));
+    }
     if (report) {
         report[0] = def_us;
         report[1] = tuned_us;
@@ -2750,13 +2851,17 @@ gpe_status gpe_tune(const gpe_config* cfg, int workload, const char* cache_path,
 
 gpe_status gpe_set_flow(gpe_handle* h, int on, unsigned wait_bound) {
     GPE_TRY(check_handle(h));
-    if (on != 0 && on != 1) return fail(GPE_ERR_INVALID_ARG, "on must be 0 or 1");
+    if (on < 0 || on > 2) return fail(GPE_ERR_INVALID_ARG, "mode must be 0, 1 or 2");
     GPE_TRY(flow_enable(h, on, wait_bound));
     GPE_CUDA(cudaStreamSynchronize(h->st));
     return GPE_OK;
 }
 
-int gpe_flow_active(const gpe_handle* h) { return h && flow_usable(h) ? 1 : 0; }
+int gpe_flow_active(const gpe_handle* h) {
+    if (!h) return 0;
+    if (flow_usable(h)) return 1;
+    return flow_strided_usable(h, h->nf) && h->ny > 1 && h->nz > 1 ? 2 : 0;
+}
 
 gpe_status gpe_flow_status(gpe_handle* h, int* status_out) {
     GPE_TRY(check_handle(h));

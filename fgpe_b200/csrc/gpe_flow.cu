@@ -39,6 +39,25 @@ int flow_ctas_per_sm(int L) {
     return 0;
 }
 
+int flow_strided_ctas_per_sm(int L) {
+#define GPE_FLOW_SOCC(N) \
+    if (L == N) return flow_strided_occupancy<N>();
+    GPE_FLOW_LENGTHS(GPE_FLOW_SOCC)
+#undef GPE_FLOW_SOCC
+    return 0;
+}
+
+bool dispatch_flow_strided(int L, const FlowArgs& fa, int grid, cudaStream_t st, cudaError_t* err) {
+#define GPE_FLOW_SCASE(N)                            \
+    if (L == N) {                                    \
+        *err = launch_flow_strided<N>(fa, grid, st); \
+        return true;                                 \
+    }
+    GPE_FLOW_LENGTHS(GPE_FLOW_SCASE)
+#undef GPE_FLOW_SCASE
+    return false;
+}
+
 bool dispatch_flow(int L, bool obs, const FlowArgs& fa, int grid, cudaStream_t st, cudaError_t* err) {
 #define GPE_FLOW_CASE(N)                                                                       \
     if (L == N) {                                                                              \

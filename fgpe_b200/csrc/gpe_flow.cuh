@@ -100,6 +100,56 @@ __device__ __forceinline__ void flow_deps(unsigned* cnt, unsigned s, unsigned pa
     }
 }
 
+// Launch prologue of the persistent kernels: waits for the previous grid
+// (its memory is then visible), and CTA 0 zeroes the counter set of the
+// next launch, which the previous launch used.  False when an earlier wait
+// gave up (the launch then does nothing).
+__device__ __forceinline__ bool flow_begin(FlowSync* sy, int set) {
+    pass_prologue_sync();
+    if (flow_ld_i(&sy->status) != 0) return false;
+    if (blockIdx.x == 0) {
+        unsigned* other = &sy->cnt[set ^ 1][0][0];
+        for (int i = threadIdx.x; i < 4 * FLOW_MAXC; i += FLOW_THREADS) other[i] = 0u;
+        if (threadIdx.x == 0) sy->ticket[set ^ 1] = 0u;
+    }
+    return true;
+}
+
+// Thread 0's part of taking a tile: `next` is the tile reserved earlier; the
+// one after it is reserved now, then the wait for *w >= need (w null: no
+// wait), bounded; an expired wait records GPE_ERR_TIMEOUT in the step's and
+// the handle's status words.  Returns the tile, or `total` when the launch
+// is over for this CTA.
+__device__ __forceinline__ unsigned flow_take(FlowSync* sy, int set, unsigned& next, unsigned total, const unsigned* w,
+                                              unsigned need, unsigned bound, int* hstatus) {
+    const unsigned item = next;
+    if (item >= total || flow_ld_i(&sy->status) != 0) return total;
+    next = atomicAdd(&sy->ticket[set], 1u);
+    if (w != nullptr && flow_ld(w) < need) {
+        unsigned it = 0;
+        while (flow_ld(w) < need) {
+            if (++it > bound || flow_ld_i(&sy->status) != 0) {
+                atomicExch(&sy->status, (int)GPE_ERR_TIMEOUT);
+                atomicExch(hstatus, (int)GPE_ERR_TIMEOUT);
+                return total;
+            }
+            __nanosleep(32);
+        }
+    }
+    __threadfence();  // acquire: the tiles counted in *w are visible
+    return item;
+}
+
+// After a tile: every thread's stores are issued (barrier), then one fence
+// and the count (release).
+__device__ __forceinline__ void flow_done(unsigned* done) {
+    __syncthreads();
+    if (threadIdx.x == 0 && done != nullptr) {
+        __threadfence();
+        atomicAdd(done, 1u);
+    }
+}
+
 // OBS: the step returns the logging observables, so stage 4's x tiles run
 // the reducing epilogue (XK_RKO: the last tile finalises, no x forward of
 // the new state) instead of XK_RKF.
@@ -108,58 +158,32 @@ __global__ void __launch_bounds__(FLOW_THREADS, FLOW_MIN_BLOCKS) k_flow_step(con
     typedef FlowGeom<L> G;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned s_item;
-    __shared__ int s_go;
     constexpr unsigned NT = G::NTX;
     constexpr unsigned N1 = NT * L, N2 = NT * L, N3 = NT * L, N4 = (L * L) / G::ROWS;
     constexpr unsigned NS = N1 + N2 + N3 + N4, TOTAL = 4 * NS;
     FlowSync* sy = fa.sync;
     const int set = fa.set;
     unsigned* cnt = &sy->cnt[set][0][0];
-
-    // the previous launch (the previous step, or the pass that filled W) is
-    // complete and visible after this wait
-    pass_prologue_sync();
-    if (flow_ld_i(&sy->status) != 0) return;
-    if (blockIdx.x == 0) {  // the next launch's set: the previous launch used it and is done
-        unsigned* other = &sy->cnt[set ^ 1][0][0];
-        for (int i = threadIdx.x; i < 4 * FLOW_MAXC; i += FLOW_THREADS) other[i] = 0u;
-        if (threadIdx.x == 0) sy->ticket[set ^ 1] = 0u;
-    }
+    if (!flow_begin(sy, set)) return;
 
     unsigned next = 0;
     if (threadIdx.x == 0) next = atomicAdd(&sy->ticket[set], 1u);
     for (;;) {
         if (threadIdx.x == 0) {
             const unsigned item = next;
-            int go = item < TOTAL && flow_ld_i(&sy->status) == 0;
-            if (go) {
-                next = atomicAdd(&sy->ticket[set], 1u);  // one tile ahead
+            unsigned* w = nullptr;
+            unsigned need = 0;
+            if (item < TOTAL) {
                 const unsigned s = item / NS, r = item % NS;
                 const unsigned pass = r < N1 ? 0u : (r < N1 + N2 ? 1u : (r < N1 + N2 + N3 ? 2u : 3u));
                 const unsigned j = pass == 0 ? r : (pass == 1 ? r - N1 : (pass == 2 ? r - N1 - N2 : r - N1 - N2 - N3));
-                unsigned* w;
-                unsigned need;
                 flow_deps<L>(cnt, s, pass, j, &w, &need);
-                if (w != nullptr && flow_ld(w) < need) {
-                    unsigned it = 0;
-                    while (flow_ld(w) < need) {
-                        if (++it > fa.wait_bound || flow_ld_i(&sy->status) != 0) {
-                            atomicExch(&sy->status, (int)GPE_ERR_TIMEOUT);
-                            atomicExch(&fa.x[0].sc->status, (int)GPE_ERR_TIMEOUT);  // the handle's status word
-                            go = 0;
-                            break;
-                        }
-                        __nanosleep(32);
-                    }
-                }
-                __threadfence();
             }
-            s_item = item;
-            s_go = go;
+            s_item = flow_take(sy, set, next, TOTAL, w, need, fa.wait_bound, &fa.x[0].sc->status);
         }
         __syncthreads();
-        if (!s_go) break;
         const unsigned item = s_item;
+        if (item >= TOTAL) break;
         const unsigned s = item / NS, r = item % NS;
         unsigned* done;
         if (r < N1) {
@@ -182,11 +206,47 @@ __global__ void __launch_bounds__(FLOW_THREADS, FLOW_MIN_BLOCKS) k_flow_step(con
                 xpass_tile<float, L, 1, XK_RKF, BuiltinHam>(fa.x[s], G::ROWS, j, 0u, N4, smem_raw);
             done = cnt + 3 * FLOW_MAXC + (j * G::ROWS) / L;
         }
-        __syncthreads();  // the tile's stores are issued; the exchange storage is free
+        flow_done(done);  // also frees the exchange storage for the next tile
+    }
+}
+
+// Mode 2: the three strided passes of one stage (y forward, z forward *
+// k-space * inverse, y inverse) in one launch, the x passes staying their
+// own launches.  All three lists are x-block major and each pass depends on
+// the previous one per x block only (the z tiles of block xb need its y
+// forward tiles of every plane, the y-inverse tiles of xb its z tiles of
+// every row), so the tiles stream without a corner turn: the z tiles of
+// block 0 start once the first L y-forward tiles are done.  Registers: the
+// paired strided tile alone (72, seven CTAs per SM).
+constexpr int FLOW_S_MIN_BLOCKS = 7;
+
+template <int L>
+__global__ void __launch_bounds__(FLOW_THREADS, FLOW_S_MIN_BLOCKS) k_flow_strided(const __grid_constant__ FlowArgs fa) {
+    typedef FlowGeom<L> G;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ unsigned s_item;
+    constexpr unsigned NT = G::NTX, NP = NT * L, TOTAL = 3 * NP;
+    FlowSync* sy = fa.sync;
+    const int set = fa.set;
+    unsigned* cnt = &sy->cnt[set][0][0];
+    if (!flow_begin(sy, set)) return;
+
+    unsigned next = 0;
+    if (threadIdx.x == 0) next = atomicAdd(&sy->ticket[set], 1u);
+    for (;;) {
         if (threadIdx.x == 0) {
-            __threadfence();
-            atomicAdd(done, 1u);
+            const unsigned item = next;
+            unsigned* w = nullptr;
+            unsigned need = L;
+            if (item < TOTAL && item >= NP) w = cnt + (item < 2 * NP ? 0 : FLOW_MAXC) + (item % NP) / L;
+            s_item = flow_take(sy, set, next, TOTAL, w, need, fa.wait_bound, &fa.s[0].sc->status);
         }
+        __syncthreads();
+        const unsigned item = s_item;
+        if (item >= TOTAL) break;
+        const unsigned pass = item / NP, j = item % NP, xb = j / L, o = j % L;
+        spass2_tile<L, 1, G::TXP, 0>(fa.s[pass], (int)NT, o * NT + xb, 0u, smem_raw);
+        flow_done(pass < 2 ? cnt + pass * FLOW_MAXC + xb : nullptr);
     }
 }
 
@@ -203,6 +263,30 @@ cudaError_t launch_flow(const FlowArgs& fa, int grid, cudaStream_t st) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, k_flow_step<L, OBS>, fa);
+}
+
+template <int L>
+cudaError_t launch_flow_strided(const FlowArgs& fa, int grid, cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(FLOW_THREADS);
+    cfg.dynamicSmemBytes = FlowGeom<L>::SMEM_S;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_flow_strided<L>, fa);
+}
+
+template <int L>
+int flow_strided_occupancy() {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_flow_strided<L>, FLOW_THREADS, FlowGeom<L>::SMEM_S) !=
+        cudaSuccess)
+        return 0;
+    return n;
 }
 
 template <int L>

@@ -25,7 +25,7 @@ struct FlowSync {
 
 struct FlowArgs {
     PassArgs<float> s[3];  // y forward, z forward * k-space * inverse, y inverse
-    PassArgs<float> x[4];  // x inverse + RK4 stage 1..4 epilogue + x forward
+    PassArgs<float> x[4];  // x inverse + RK4 stage 1..4 epilogue + x forward (mode 1 only)
     FlowSync* sync;
     int set;               // counter set of this launch (launch parity)
     int ntx;               // x blocks of a strided tile row
@@ -40,6 +40,9 @@ int flow_rows(int L);
 int flow_ntx(int L);
 // Resident CTAs per SM of the flow kernel for length L (0 if none).
 int flow_ctas_per_sm(int L);
+// The three strided passes of one stage in one launch (mode 2).
+int flow_strided_ctas_per_sm(int L);
+bool dispatch_flow_strided(int L, const FlowArgs& fa, int grid, cudaStream_t st, cudaError_t* err);
 // obs: the step's stage 4 runs the reducing epilogue (logging observables).
 bool dispatch_flow(int L, bool obs, const FlowArgs& fa, int grid, cudaStream_t st, cudaError_t* err);
 

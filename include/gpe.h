@@ -412,8 +412,8 @@ gpe_status gpe_norm_noalloc(const void* dev_psi_c128, long long n, double dv, do
  * same key; NULL = do not store).  report (may be NULL) receives 12 values:
  * default and tuned microseconds per step, variants timed, the chosen
  * variants s[axis 1][mode 0..2], s[axis 2][mode 0..2], the rows, the
- * fused y-z flag and the persistent-step flag (gpe_set_flow; real-time
- * workload only). */
+ * fused y-z flag and the persistent mode (gpe_set_flow: 1 only for the
+ * real-time workload, 2 for either). */
 gpe_status gpe_tune(const gpe_config* cfg, int workload, const char* cache_path, double* report);
 /* Process-wide: gpe_create and gpe_batch_create apply the cache line that
  * matches a new handle (or batch group); NULL = read $GPE_TUNE_CACHE if set. */
@@ -452,7 +452,16 @@ int        gpe_pass_variant_exists(const gpe_config* cfg, int axis, int v);
  * observables) and in the step's own status word, after which later
  * persistent steps do nothing until gpe_flow_status re-arms them. */
 gpe_status gpe_set_flow(gpe_handle* h, int on, unsigned wait_bound);
-/* 1 when the handle's real-time steps run as the persistent step. */
+/* on = 2 (persistent strided stage): the three strided passes of every
+ * one-field complex64 pass chain of a cubic 128 or 256 grid (real- and
+ * imaginary-time steps, apply-H, observables) run as one launch per stage
+ * whose CTAs stream the y-forward, z forward*k-space*inverse and y-inverse
+ * tiles of each x block, every tile waiting only for the tiles of its x
+ * block that it reads (the x passes keep their own launches); results equal
+ * the chain with the default radix order bit for bit.  The same wait bound,
+ * timeout status and re-arm apply. */
+/* 1 when the handle's real-time steps run as the persistent step, 2 when its
+ * strided stages run as one launch each, 0 otherwise. */
 int        gpe_flow_active(const gpe_handle* h);
 /* Synchronises; *status_out = 0 or GPE_ERR_TIMEOUT (a persistent step gave
  * up since the last call).  After a timeout the counters and both status
@@ -466,12 +475,14 @@ long long  gpe_kernel_launches(const gpe_handle* h);
 
 /* ---- measurement (no counterpart in the reference, whose only timing is
  * unsynchronised host chrono, src/oneComponentGPSolver.cu:153,197-200) ----- */
-#define GPE_PROF_KINDS 7
+#define GPE_PROF_KINDS 8
 #define GPE_PROF_FLOW 6
+#define GPE_PROF_SFLOW 7
 /* Pass kinds: 0 x-forward (+prologue), 1 x-inverse (+epilogue), 2 x-full,
  * 3 strided forward, 4 strided inverse, 5 strided forward*k-space*inverse
  * (with the fused y-z kernel: that kernel, and no kinds 3 and 4), 6 the
- * persistent RK4 step (gpe_set_flow: one launch for the whole step). */
+ * persistent RK4 step (gpe_set_flow mode 1: one launch for the whole step),
+ * 7 the persistent strided stage (mode 2: the three strided passes). */
 /* When enabled, every pass launch is bracketed by CUDA events on the
  * handle's stream. */
 gpe_status gpe_profile_enable(gpe_handle* h, int enable);

@@ -122,3 +122,52 @@ def test_flow_timeout_is_reported_and_rearmed(gpu):
         s.step_real(0, 2)
         assert s.flow_status() == 0
         assert np.array_equal(s.get_psi(0), ref)
+
+
+def run_mode2(cfg, V, psi, mode, bound=0):
+    """Real-time steps (with and without observables), then imaginary-time
+    iterations of cfg's scheme, through one handle; psi and observables."""
+    with Solver(cfg) as s:
+        s.set_vext(0, V)
+        s.set_psi(0, psi)
+        s.set_flow(mode, bound)
+        o1 = s.step_real(0, 3, want_obs=True)
+        s.step_real(3, 2)
+        p1 = s.get_psi(0)
+        o2 = s.observables(0.0)
+        s.step_imag(0, 5)
+        return p1, o1, o2, s.get_psi(0), s.flow_active
+
+
+@pytest.mark.parametrize("n", [128, 256])
+@pytest.mark.parametrize("scheme", ["heavyball", "rk4"])
+def test_strided_stage_equals_the_chain_bit_for_bit(gpu, n, scheme):
+    from fgpe_b200 import IMAG_HEAVYBALL, IMAG_RK4
+    prms = np.zeros(32)
+    prms[0:3] = 1100.0 / (4 * PI_REF)
+    cfg = make_config((n, n, n), 10.0, dt=5e-4, precision=C64, prms=prms, beta=0.9,
+                      imag_scheme=IMAG_HEAVYBALL if scheme == "heavyball" else IMAG_RK4)
+    V, psi = start(cfg)
+    a = run_mode2(cfg, V, psi, 2)
+    b = run_mode2(cfg, V, psi, 0)
+    assert a[4] == 2 and b[4] == 0
+    for x, y in zip(a[:4], b[:4]):
+        assert np.array_equal(x, y)
+
+
+def test_strided_stage_timeout_is_reported_and_rearmed(gpu):
+    cfg = quench_cfg(128)
+    V, psi = start(cfg)
+    ref, _, _, _ = run(cfg, V, psi, False, [(2, False)])
+    with Solver(cfg) as s:
+        s.set_vext(0, V)
+        s.set_psi(0, psi)
+        s.set_flow(2, 1)
+        s.step_real(0, 2)
+        assert s.flow_status() == GPE_ERR_TIMEOUT
+        assert s.flow_status() == 0
+        s.set_flow(2, 1 << 22)
+        s.set_psi(0, psi)
+        s.step_real(0, 2)
+        assert s.flow_status() == 0
+        assert np.array_equal(s.get_psi(0), ref)
