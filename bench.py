@@ -128,7 +128,8 @@ def cached_or_tune(cfg, workload, cache):
                     (cfg.nx, cfg.ny, cfg.nz, cfg.precision, nf, 1):
                 return {"default_us": d["default_us"], "tuned_us": d["tuned_us"], "from_cache": cache,
                         "variants": [d[k] for k in ("s10", "s11", "s12", "s20", "s21", "s22")],
-                        "xrows": d["xrows"], "yz": d.get("yz", 0), "flow": d.get("flow", 0)}
+                        "xrows": d["xrows"], "yz": d.get("yz", 0), "flow": d.get("flow", 0),
+                        "xstage": d.get("xstage", 0)}
     return gp.tune(cfg, workload, cache)
 
 

@@ -140,6 +140,8 @@ def lib() -> ctypes.CDLL:
         "gpe_set_flow": (c_int, [H, c_int, ctypes.c_uint]),
         "gpe_flow_active": (c_int, [H]),
         "gpe_flow_status": (c_int, [H, POINTER(c_int)]),
+        "gpe_set_x_staging": (c_int, [H, c_int]),
+        "gpe_x_staging": (c_int, [H]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -214,11 +216,11 @@ def tune(cfg: GPEConfig, workload: int = 0, cache_path: str | None = None) -> di
     """Autotune the pass variants of cfg's grid (gpe_tune): workload 0 =
     real-time RK4 steps, 1 = imaginary-time iterations.  Stores the result
     in the JSON-lines cache_path when given."""
-    rep = np.zeros(12)
+    rep = np.zeros(13)
     _check(lib().gpe_tune(byref(cfg), workload, cache_path.encode() if cache_path else None, _dp(rep)))
     return {"default_us": float(rep[0]), "tuned_us": float(rep[1]), "timed": int(rep[2]),
             "variants": [int(x) for x in rep[3:9]], "xrows": int(rep[9]), "yz": int(rep[10]),
-            "flow": int(rep[11])}
+            "flow": int(rep[11]), "xstage": int(rep[12])}
 
 
 def set_tune_cache(path: str | None) -> None:
@@ -419,6 +421,15 @@ class Solver:
         one launch, False / 0 = the per-pass chain; wait_bound 0 keeps the
         current bound."""
         _check(lib().gpe_set_flow(self._h, int(mode), int(wait_bound)))
+
+    def set_x_staging(self, on: bool) -> None:
+        """Stage the fused real-time x pass's epilogue inputs in shared memory
+        (gpe_set_x_staging; complex64 one-field chains)."""
+        _check(lib().gpe_set_x_staging(self._h, 1 if on else 0))
+
+    @property
+    def x_staging(self) -> bool:
+        return bool(lib().gpe_x_staging(self._h))
 
     @property
     def flow_active(self) -> int:

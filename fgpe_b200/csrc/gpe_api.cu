@@ -94,6 +94,9 @@ struct gpe_handle {
     // one persistent launch per step (k_flow_step, gpe_flow.cuh); its
     // dependency counters, the launch parity and the wait bound
     int flow = 0;
+    // 1: the fused real-time RK x pass of a complex64 one-field chain stages
+    // its epilogue inputs in shared memory (XK_RKS)
+    int xstage = 0;
     FlowSync* flow_sync = nullptr;
     long long flow_launches = 0;
     unsigned flow_bound = 1u << 22;
@@ -490,6 +493,7 @@ PassArgs<R> base_args(gpe_handle* h) {
     a.nbatch = h->nb;
     a.bstride = h->nb > 1 ? h->N : 0;
     a.pstride = (long long)h->ny * h->nz * MAXQ * 2;
+    a.xstage = h->xstage;
     return a;
 }
 
@@ -2541,7 +2545,7 @@ std::string tune_line(const gpe_handle* h, double def_us, double tuned_us) {
       << ",\"nf\":" << k.nf << ",\"nb\":" << k.nb;
     for (int ax = 1; ax <= 2; ++ax)
         for (int m = 0; m < 3; ++m) o << ",\"s" << ax << m << "\":" << h->svar[ax][m];
-    o << ",\"xrows\":" << h->xrows << ",\"yz\":" << h->yz << ",\"flow\":" << h->flow;
+    o << ",\"xrows\":" << h->xrows << ",\"yz\":" << h->yz << ",\"flow\":" << h->flow << ",\"xstage\":" << h->xstage;
     char buf[64];
     std::snprintf(buf, sizeof(buf), ",\"default_us\":%.3f,\"tuned_us\":%.3f}", def_us, tuned_us);
     o << buf;
@@ -2572,6 +2576,8 @@ void tune_apply_cache(gpe_handle* h) {
     if (json_int(hit, "xrows", &r) && r >= 0 && r <= 256) h->xrows = r;
     int yz = 0;
     if (json_int(hit, "yz", &yz) && (yz == 0 || (yz == 1 && yz_usable(h, h->nf)))) h->yz = yz;
+    int xs = 0;
+    if (json_int(hit, "xstage", &xs) && (xs == 0 || xs == 1)) h->xstage = xs;
     int fl = 0;
     if (json_int(hit, "flow", &fl) && ((fl == 1 && flow_eligible(h)) || fl == 2)) flow_enable(h, fl, 0);
 }
@@ -2719,7 +2725,9 @@ gpe_status tune_handle_t(gpe_handle* h, int workload, double* report) {
     const int rmax = (256 / T) > 0 ? 256 / T : 1;
     int best_r = 0;
     double best_us = 1e30;
-    for (int r = rmax; r >= 1 && r >= rmax / 2; --r) {
+    // down to a quarter of the longest tile: at 128 (16 threads a row) four
+    // rows make 64-thread CTAs, sixteen of which fill an SM's 64 warps
+    for (int r = rmax; r >= 1 && r >= rmax / 4; --r) {
         h->xrows = (r == rmax) ? 0 : r;
         double us = 0.0;
         GPE_TRY(time_steps<R>(h, workload, &us));
@@ -2744,6 +2752,33 @@ gpe_status tune_handle_t(gpe_handle* h, int workload, double* report) {
     }
     double tuned_us = 0.0;
     GPE_TRY(time_steps<R>(h, workload, &tuned_us));
+    // real-time complex64 one-field chains: the fused x pass with staged
+    // epilogue inputs, at the chosen rows and at half and a quarter of the
+    // longest tile (staging takes shared memory, so fewer rows may pay)
+    if (workload == 0 && h->prec == GPE_C64 && h->nf == 1 && h->nb == 1 && (h->ny > 1 || h->nz > 1)) {
+        const int rows0 = h->xrows;
+        const int rtry[3] = {rows0, rmax / 2, rmax / 4};
+        int best_rows = rows0;
+        bool keep = false;
+        for (int k = 0; k < 3; ++k) {
+            if (rtry[k] < 0 || (k > 0 && (rtry[k] < 1 || rtry[k] == rows0))) continue;
+            h->xstage = 1;
+            h->xrows = rtry[k];
+            double us = 0.0;
+            const gpe_status s = time_steps<R>(h, workload, &us);
+            ++timed;
+            if (s == GPE_OK && us < tuned_us * 0.99) {
+                tuned_us = us;
+                best_rows = rtry[k];
+                keep = true;
+            } else {
+                cudaGetLastError();
+            }
+        }
+        h->xstage = keep ? 1 : 0;
+        h->xrows = keep ? best_rows : rows0;
+        GPE_CUDA(cudaStreamSynchronize(h->st));
+    }
     // real-time steps as one persistent launch each (same arithmetic)
     if (workload == 0 && flow_eligible(h)) {
         double us = 0.0;
@@ -2803,6 +2838,7 @@ gpe_status tune_config(const gpe_config* cfg, int nb, int workload, double* repo
     h->xrows = 0;
     h->yz = 0;
     h->flow = 0;
+    h->xstage = 0;
     gpe_status s = h->prec == GPE_C64 ? tune_handle_t<float>(h, workload, report)
                                       : tune_handle_t<double>(h, workload, report);
     if (s != GPE_OK) {
@@ -2842,6 +2878,7 @@ gpe_status gpe_tune(const gpe_config* cfg, int workload, const char* cache_path,
         report[9] = h->xrows;
         report[10] = h->yz;
         report[11] = h->flow;
+        report[12] = h->xstage;
     }
     cudaStreamSynchronize(h->st);
     free_all(h);
@@ -2856,6 +2893,15 @@ gpe_status gpe_set_flow(gpe_handle* h, int on, unsigned wait_bound) {
     GPE_CUDA(cudaStreamSynchronize(h->st));
     return GPE_OK;
 }
+
+gpe_status gpe_set_x_staging(gpe_handle* h, int on) {
+    GPE_TRY(check_handle(h));
+    if (on != 0 && on != 1) return fail(GPE_ERR_INVALID_ARG, "on must be 0 or 1");
+    h->xstage = on;
+    return GPE_OK;
+}
+
+int gpe_x_staging(const gpe_handle* h) { return h ? h->xstage : 0; }
 
 int gpe_flow_active(const gpe_handle* h) {
     if (!h) return 0;

@@ -50,9 +50,14 @@ enum SpecOp { SPEC_NONE = 0, SPEC_KIN = 1, SPEC_PX = 2 };
 // XK_RKF is XK_RK followed by the forward x transform of the state it just
 // wrote, which is the x-forward pass of the next stage.
 // XK_ADJ is the adjoint stage epilogue of the control gradient.
+// XK_RKS is XK_RKF with the epilogue inputs staged: every thread copies the
+// values its epilogue will read (V, the stage state, the accumulator, psi0,
+// the low part) into its own shared-memory slots with asynchronous copies at
+// kernel start, before the wait on the previous pass, so that they are in
+// flight during the inverse transform (complex64, one field).
 enum XKind { XK_FWD = 0, XK_STORE = 1, XK_RK = 2, XK_HB = 3, XK_RKI = 4, XK_AH = 5, XK_FULL = 6, XK_RKO = 7,
-             XK_RKF = 8, XK_ADJ = 9 };
-constexpr int NXKIND = 10;  // SPEC_PX: BECVPx, src/parallel.cu:283-292
+             XK_RKF = 8, XK_ADJ = 9, XK_RKS = 10 };
+constexpr int NXKIND = 11;  // SPEC_PX: BECVPx, src/parallel.cu:283-292
 
 constexpr int MAXQ = 6;       // reduced quantities per launch (3 per component)
 template <typename R>
@@ -67,6 +72,7 @@ struct PassArgs {
     int check_done;          // exit when sc->done is set (stepping chunks)
     int want_obs;            // RK stage 4: logging reductions
     int fuse_fwd;            // RK epilogue: also x-forward transform the new state into w
+    int xstage;              // complex64 fused RK epilogue: stage its inputs (XK_RKS)
     // Batched instances (gpe_batch): blockIdx.y selects the instance; its
     // fields sit bstride elements apart, its d_h_params, scalars and partial
     // sums at prms + 32*inst, sc + inst, partials + pstride*inst.

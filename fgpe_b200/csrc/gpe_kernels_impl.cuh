@@ -401,6 +401,30 @@ __device__ __forceinline__ EpiIn<typename Cx<R>::T> load_inputs(const PassArgs<R
     }
 }
 
+// XK_RKS: where a tile's staged epilogue inputs start in shared memory
+// (after the exchange rows, 16-byte aligned), and the inputs of register e
+// read back from this thread's slots (field f of register e at
+// stg[(f * E + e) * blockDim.x + threadIdx.x]; fields V, the stage state,
+// the accumulator, psi0, the low part, as stage_rk_inputs copies them).
+template <typename C>
+__host__ __device__ constexpr size_t xstage_offset(int rows, int L) {
+    return ((size_t)rows * xpad(L) * sizeof(C) + 15) / 16 * 16;
+}
+template <typename C, int E, int STG>
+__device__ __forceinline__ EpiIn<C> staged_inputs(const PassArgs<float>& a, const C* stg, int e) {
+    EpiIn<C> in;
+    const unsigned n = blockDim.x, i = threadIdx.x;
+    in.V[0] = stg[(0 * E + e) * n + i];
+    in.psi[0] = stg[(1 * E + e) * n + i];
+    if constexpr (STG > 1) {
+        in.k[0] = stg[(2 * E + e) * n + i];
+        in.p0[0] = stg[(3 * E + e) * n + i];
+    }
+    if constexpr (STG == 4)
+        if (a.lo[0] != nullptr) in.xo[0] = stg[(4 * E + e) * n + i];
+    return in;
+}
+
 // v: the NF inverse-transformed fields at global index gi (kinetic part per
 // psi component, dipolar potential field last); in: the loaded inputs.
 // For EPI_RK, nv receives the new state of each component (the value stored
@@ -621,10 +645,11 @@ __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const typen
 // FUSE: v[f][e] is replaced by the new RK state of component f (and, for the
 // dipolar density field, its |psi|^2), ready for the forward x transform.
 template <typename R, int NF, int EPI, bool MAYRED, int L, int E, int T, int Rr, bool FUSE = false, int STG = 0,
-          class H = BuiltinHam>
+          class H = BuiltinHam, bool STAGED = false>
 __device__ __forceinline__ void epilogue_line(const PassArgs<R>& a, const typename H::template Coef<R>& hc,
                                               const PsiScale<R>& ps,
-                                              typename Cx<R>::T (&v)[NF][E], long long g0, int cur, DD* acc) {
+                                              typename Cx<R>::T (&v)[NF][E], long long g0, int cur, DD* acc,
+                                              const typename Cx<R>::T* stg = nullptr) {
     typedef typename Cx<R>::T C;
     constexpr bool LO = EPI == EPI_RK && sizeof(R) == 4 && (STG == 4 || STG == 0);  // may read the low part
     constexpr int EC0 = (NF > 1) ? 1 : ((EPI == EPI_ADJ || LO) ? 2 : 4);
@@ -633,8 +658,14 @@ __device__ __forceinline__ void epilogue_line(const PassArgs<R>& a, const typena
     for (int e0 = 0; e0 < E; e0 += EC) {
         EpiIn<C> in[EC];
 #pragma unroll
-        for (int j = 0; j < EC; ++j)
-            in[j] = load_inputs<R, EPI, NF, STG>(a, ps, g0 + reg_off<L, E, T, Rr>(e0 + j), cur);
+        for (int j = 0; j < EC; ++j) {
+            if constexpr (STAGED) {
+                static_assert(sizeof(R) == 4 && NF == 1 && EPI == EPI_RK && STG != 0, "staged inputs: XK_RKS only");
+                in[j] = staged_inputs<C, E, STG>(a, stg, e0 + j);
+            } else {
+                in[j] = load_inputs<R, EPI, NF, STG>(a, ps, g0 + reg_off<L, E, T, Rr>(e0 + j), cur);
+            }
+        }
 #pragma unroll
         for (int j = 0; j < EC; ++j) {
             C tmp[NF];
@@ -659,7 +690,8 @@ __device__ __forceinline__ void epilogue_line(const PassArgs<R>& a, const typena
 template <typename R, int NF, int KIND, int L, int E, int T, int Rr, class H = BuiltinHam>
 __device__ __forceinline__ void epilogue_dispatch(const PassArgs<R>& a, const typename H::template Coef<R>& hc,
                                                   const PsiScale<R>& ps,
-                                                  typename Cx<R>::T (&v)[NF][E], long long g0, int cur, DD* acc) {
+                                                  typename Cx<R>::T (&v)[NF][E], long long g0, int cur, DD* acc,
+                                                  const typename Cx<R>::T* stg = nullptr) {
 #define GPE_EPI(OP, RED) epilogue_line<R, NF, OP, RED, L, E, T, Rr, false, 0, H>(a, hc, ps, v, g0, cur, acc)
     if constexpr (KIND == XK_STORE) GPE_EPI(EPI_STORE, false);
     else if constexpr (KIND == XK_RK) GPE_EPI(EPI_RK, false);
@@ -668,6 +700,13 @@ __device__ __forceinline__ void epilogue_dispatch(const PassArgs<R>& a, const ty
         if (a.stage == 1) epilogue_line<R, NF, EPI_RK, false, L, E, T, Rr, true, 1, H>(a, hc, ps, v, g0, cur, acc);
         else if (a.stage < 4) epilogue_line<R, NF, EPI_RK, false, L, E, T, Rr, true, 2, H>(a, hc, ps, v, g0, cur, acc);
         else epilogue_line<R, NF, EPI_RK, false, L, E, T, Rr, true, 4, H>(a, hc, ps, v, g0, cur, acc);
+    } else if constexpr (KIND == XK_RKS) {
+        if (a.stage == 1)
+            epilogue_line<R, NF, EPI_RK, false, L, E, T, Rr, true, 1, H, true>(a, hc, ps, v, g0, cur, acc, stg);
+        else if (a.stage < 4)
+            epilogue_line<R, NF, EPI_RK, false, L, E, T, Rr, true, 2, H, true>(a, hc, ps, v, g0, cur, acc, stg);
+        else
+            epilogue_line<R, NF, EPI_RK, false, L, E, T, Rr, true, 4, H, true>(a, hc, ps, v, g0, cur, acc, stg);
     } else if constexpr (KIND == XK_RKO) {  // launched for stage 4 only
         epilogue_line<R, NF, EPI_RK, true, L, E, T, Rr, false, 4, H>(a, hc, ps, v, g0, cur, acc);
     }
@@ -720,7 +759,7 @@ __host__ __device__ constexpr int pass_min_blocks() {
 // one-field real-time RK roles fit 64 registers: one CTA more.
 template <typename R, int L, int NF, int KIND>
 __host__ __device__ constexpr int xpass_min_blocks() {
-    return (NF == 1 && (KIND == XK_RKF || KIND == XK_RK) && pass_min_blocks<R, L, NF>() == 3)
+    return (NF == 1 && (KIND == XK_RKF || KIND == XK_RK || KIND == XK_RKS) && pass_min_blocks<R, L, NF>() == 3)
                ? 4
                : (kind_reduces<KIND>() && pass_min_blocks<R, L, NF>() > 1 ? pass_min_blocks<R, L, NF>() - 1
                                                                            : pass_min_blocks<R, L, NF>());
@@ -837,8 +876,15 @@ __device__ __forceinline__ void xpass_tile(const PassArgs<R>& a, int rows, unsig
         const typename H::template Coef<R> hc = H::template coef<R>(a, ip.prms);
 #pragma unroll
         for (int f = 0; f < NF; ++f) line_fft_inv<L>(v[f], addr, a.tw, t);
-        if (valid) epilogue_dispatch<R, NF, KIND, L, E, T, RinF, H>(a, hc, ps, v, g0, cur, acc);
-        if constexpr (KIND == XK_RKF) {
+        if constexpr (KIND == XK_RKS) {
+            // this thread's staged inputs (issued at kernel start) have landed
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            const C* stg = reinterpret_cast<const C*>(smem_raw + xstage_offset<C>(rows, L));
+            if (valid) epilogue_dispatch<R, NF, KIND, L, E, T, RinF, H>(a, hc, ps, v, g0, cur, acc, stg);
+        } else {
+            if (valid) epilogue_dispatch<R, NF, KIND, L, E, T, RinF, H>(a, hc, ps, v, g0, cur, acc);
+        }
+        if constexpr (KIND == XK_RKF || KIND == XK_RKS) {
             // next stage's x-forward pass on the state just written (in place on w)
 #pragma unroll
             for (int f = 0; f < NF; ++f) line_fft_fwd<L>(v[f], addr, a.tw, t);
@@ -859,10 +905,47 @@ __device__ __forceinline__ void xpass_tile(const PassArgs<R>& a, int rows, unsig
     }
 }
 
+// XK_RKS: each thread copies the epilogue inputs of its E points (V and the
+// stage state; from stage 2 the accumulator and psi0; at stage 4 the low
+// part) from global memory into its own shared-memory slots with 8-byte
+// asynchronous copies (one group), in the order staged_inputs reads them.
+// Each thread reads back only what it copied itself, so the wait for its own
+// group is all the synchronisation needed.
+template <typename R, int L>
+__device__ __forceinline__ void stage_rk_inputs(const PassArgs<R>& a, int rows, unsigned char* smem_raw) {
+    typedef typename Cx<R>::T C;
+    static_assert(sizeof(C) == 8, "staged inputs: complex64 only");
+    constexpr int E = Plan<L>::E;
+    constexpr int T = Plan<L>::T;
+    constexpr int RinF = Plan<L>::in_radix(false);
+    const long long boff = select_instance(a).boff;
+    const unsigned b = threadIdx.x / T, t = threadIdx.x % T;
+    const int row = (int)blockIdx.x * rows + (int)b;
+    if (row < a.nrows) {
+        const long long g0 = boff + (long long)row * L + t;
+        C* stg = reinterpret_cast<C*>(smem_raw + xstage_offset<C>(rows, L));
+        const int nfs = a.stage == 1 ? 2 : ((a.stage == 4 && a.lo[0] != nullptr) ? 5 : 4);
+        const unsigned n = blockDim.x, i = threadIdx.x;
+        for (int f = 0; f < nfs; ++f) {
+            const C* src = f == 0 ? a.vext[0] : (f == 1 ? a.pin[0] : (f == 2 ? a.kacc[0] : (f == 3 ? a.buf[0][0] : a.lo[0])));
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const C* gp = src + g0 + reg_off<L, E, T, RinF>(e);
+                const unsigned sa = (unsigned)__cvta_generic_to_shared(stg + (f * E + e) * n + i);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gp) : "memory");
+            }
+        }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
 template <typename R, int L, int NF, int KIND, class H = BuiltinHam>
 __global__ void __launch_bounds__(256, (xpass_min_blocks<R, L, NF, KIND>())) k_xpass(PassArgs<R> a, int rows) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    if constexpr (KIND == XK_RKF || KIND == XK_RK || KIND == XK_RKO) {
+    if constexpr (KIND == XK_RKS) {
+        // the inputs were written two or more launches earlier (see below)
+        stage_rk_inputs<R, L>(a, rows, smem_raw);
+    } else if constexpr (KIND == XK_RKF || KIND == XK_RK || KIND == XK_RKO) {
         // The epilogue inputs were written two or more launches earlier, so
         // the L2 prefetch may run before the wait for the preceding grid
         // (with programmatic launch this CTA can start during its tail);
@@ -1205,6 +1288,14 @@ cudaError_t launch_xpass(const PassArgs<R>& a, int rows, size_t smem, cudaStream
     int kind = xkind_of(a.mode, a.epi);
     if (kind == XK_RK && a.want_obs && a.stage == 4) kind = XK_RKO;
     else if (kind == XK_RK && a.fuse_fwd) kind = XK_RKF;
+    if constexpr (NF == 1 && sizeof(R) == 4 && H::builtin) {
+        if (kind == XK_RKF && a.xstage) {  // staged epilogue inputs: exchange rows + the staging slots
+            const int threads = rows * Plan<L>::T;
+            const int nfs = a.stage == 1 ? 2 : ((a.stage == 4 && a.lo[0] != nullptr) ? 5 : 4);
+            const size_t sm = xstage_offset<float2>(rows, L) + (size_t)nfs * Plan<L>::E * threads * sizeof(float2);
+            return launch_xpass_kind<R, L, NF, XK_RKS, H>(a, rows, sm, st);
+        }
+    }
     if (kind == XK_ADJ) {
         if constexpr (NF <= 2 && H::builtin) return launch_xpass_kind<R, L, NF, XK_ADJ, H>(a, rows, smem, st);
         return cudaErrorNotSupported;

@@ -409,11 +409,12 @@ gpe_status gpe_norm_noalloc(const void* dev_psi_c128, long long n, double dv, do
  * workload, 0 = real-time RK4 steps, 1 = imaginary-time iterations), keeps
  * the fastest, and stores one line keyed by (nx, ny, nz, precision, fields,
  * instances = 1) in the JSON-lines file cache_path (replacing a line of the
- * same key; NULL = do not store).  report (may be NULL) receives 12 values:
+ * same key; NULL = do not store).  report (may be NULL) receives 13 values:
  * default and tuned microseconds per step, variants timed, the chosen
  * variants s[axis 1][mode 0..2], s[axis 2][mode 0..2], the rows, the
- * fused y-z flag and the persistent mode (gpe_set_flow: 1 only for the
- * real-time workload, 2 for either). */
+ * fused y-z flag, the persistent mode (gpe_set_flow: 1 only for the
+ * real-time workload, 2 for either) and the x-staging flag
+ * (gpe_set_x_staging, real-time workload). */
 gpe_status gpe_tune(const gpe_config* cfg, int workload, const char* cache_path, double* report);
 /* Process-wide: gpe_create and gpe_batch_create apply the cache line that
  * matches a new handle (or batch group); NULL = read $GPE_TUNE_CACHE if set. */
@@ -467,6 +468,16 @@ int        gpe_flow_active(const gpe_handle* h);
  * up since the last call).  After a timeout the counters and both status
  * words are reset; the fields hold the partial step and must be set again. */
 gpe_status gpe_flow_status(gpe_handle* h, int* status_out);
+
+/* on = 1: the fused x-inverse pass of a complex64 one-field real-time RK4
+ * stage copies its epilogue inputs (V, the stage state, the accumulator,
+ * psi0, the low part) into shared memory with asynchronous copies at kernel
+ * start, before its wait on the previous pass, so that they are in flight
+ * during the inverse transform instead of being loaded after it; results
+ * are unchanged bit for bit.  Other handles ignore it.  A tuner variant
+ * (cache key xstage), off by default. */
+gpe_status gpe_set_x_staging(gpe_handle* h, int on);
+int        gpe_x_staging(const gpe_handle* h);
 
 /* Synchronise the handle's stream and report any asynchronous error. */
 gpe_status gpe_sync(gpe_handle* h);

@@ -226,3 +226,34 @@ def test_fused_yz_kernel_rejected_where_it_does_not_fit(gpu):
         with Solver(make_config(shape, 8.0, precision=prec)) as s:
             with pytest.raises(GPEError):
                 s.set_pass_variants([0] * 7 + [1])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(128, 128, 128), (64, 64, 64), (96, 96, 96), (256, 256, 1)])
+@pytest.mark.parametrize("rows", [0, 4])
+def test_x_staging_equals_the_unstaged_pass_bit_for_bit(gpu, shape, rows):
+    """gpe_set_x_staging: the fused real-time x pass copies its epilogue
+    inputs into shared memory before its wait instead of loading them after
+    the inverse transform; same arithmetic, so psi (high and low part) and
+    the observables must not change by a bit."""
+    prms = np.zeros(32)
+    prms[0:3] = 800.0 / (4 * PI_REF)
+    cfg = make_config(shape, 8.0, dt=5e-4, precision=C64, prms=prms, beta=0.9)
+    V = harmonic(cfg, (1.0, 1.5, 2.0))
+    psi = gaussian(cfg, width=1.3, seed=7, noise=1e-2)
+    out = {}
+    for on in (0, 1):
+        with Solver(cfg) as s:
+            s.set_vext(0, V)
+            s.set_psi(0, psi)
+            if rows:
+                v = s.pass_variants()
+                v[6] = rows
+                s.set_pass_variants(v)
+            s.set_x_staging(bool(on))
+            assert s.x_staging == bool(on)
+            s.step_real(0, 3)
+            o = s.step_real(3, 2, want_obs=True)
+            out[on] = (s.get_psi(0), o)
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
