@@ -38,13 +38,13 @@ bool GPE_NAME(dispatch_s_)(int L, const PassArgs<GPE_R>& a, int nouter, size_t s
 
 #if GPE_NF == 1
 #define GPE_SVCASE(L)                                                   \
-    case L:                                                             \
+    case L: {                                                           \
+        bool found = false;                                             \
         *err = launch_svar<GPE_R, L>(v, a, nouter, st, &found);         \
-        return found;
+        return found;                                                   \
+    }
 // Autotuner variants of the one-field strided pass at the tuned lengths.
 bool GPE_NAME(dispatch_sv_)(int L, int v, const PassArgs<GPE_R>& a, int nouter, cudaStream_t st, cudaError_t* err) {
-    bool found = false;
-    (void)found;  // families without tuned lengths have no case
     switch (L) {
         GPE_TUNED(GPE_SVCASE)
         default:
