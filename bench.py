@@ -471,10 +471,10 @@ def cpu_baseline(n, psi_gs, solvers=None, budget_s=12.0):
     return out
 
 
-def reference_cuda_build(n):
+def reference_cuda_build(n, imag=False):
     """The reference's own CUDA build (complex128, cuFFT; oracle/_ref, built
-    from its sources) timed on this GPU for the same real-time RK4 loop: a
-    comparison figure carried in the reference arm's line."""
+    from its sources) timed on this GPU for the same real-time RK4 loop (or,
+    imag, its heavy-ball imaginary-time loop): a comparison figure."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     try:
         import tempfile
@@ -483,12 +483,14 @@ def reference_cuda_build(n):
             return {"unavailable": "oracle/_ref/gpe_ref_trace not built"}
         n1, n2, rep = 200, 1200, 3
         with tempfile.TemporaryDirectory() as work:
-            trb.run(n, 10, work)
-            diffs = sorted((trb.run(n, n2, work) - trb.run(n, n1, work)) / (n2 - n1) for _ in range(rep))
+            trb.run(n, 10, work, imag)
+            diffs = sorted((trb.run(n, n2, work, imag) - trb.run(n, n1, work, imag)) / (n2 - n1)
+                           for _ in range(rep))
         per = diffs[len(diffs) // 2]
+        loop = "runImagTimeEvol" if imag else "runRealTimeEvol"
         return {"steps_per_s": round(1.0 / per, 2), "ms_per_step": round(1e3 * per, 4), "dtype": "f64",
                 "method": f"median over {rep} of loop(niter={n2}) - loop(niter={n1}), device-synchronised wall "
-                          "time of the reference's own runRealTimeEvol loop"}
+                          f"time of the reference's own {loop} loop"}
     except Exception as e:  # comparison only: never fail the arm
         return {"unavailable": str(e)[:200]}
 
@@ -1039,6 +1041,13 @@ def run_imag(args):
                 res[form]["E_rel_vs_c128_converged"] = float(abs(res[form]["E"][0] / res["c128_rk4"]["E"][0] - 1))
                 res[form]["mu_rel_vs_c128_converged"] = float(abs(res[form]["mu"][0] / res["c128_rk4"]["mu"][0] - 1))
         res["cpu_baseline"] = imag_cpu_leg(name, st)
+        if name == "ground64":
+            # the drop-in comparison: the reference's own build, heavy ball at 64^3
+            rb = reference_cuda_build(64, imag=True)
+            if "steps_per_s" in rb:
+                rb["c128_heavyball_over_reference_build"] = round(
+                    res["c128_heavyball"]["iterations_per_s"] / rb["steps_per_s"], 3)
+            res["reference_cuda_build"] = rb
         out["cases"][name] = res
     print(json.dumps(out))
 

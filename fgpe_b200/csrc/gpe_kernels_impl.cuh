@@ -278,9 +278,9 @@ __device__ void reduce_and_finalize(const PassArgs<R>& a, const InstPtr& ip, DD 
         }
         block_reduce<NQ>(s, red);
         if (threadIdx.x == 0) {
-            double S[NQ];
+            double S[MAXQ];  // quantities past NQ (one-field kernels: 3) are 0
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) S[q] = s[q].s + s[q].c;
+            for (int q = 0; q < MAXQ; ++q) S[q] = q < NQ ? s[q].s + s[q].c : 0.0;
             finalize_scalars(a, ip.sc, S);
             ip.sc->counter = 0;
             __threadfence();
@@ -809,9 +809,12 @@ __device__ __forceinline__ void xpass_tile(const PassArgs<R>& a, int rows, unsig
     const RowAddr<C, L> addr{X + b * xpad(L)};
     const int cur = ip.sc->cur_slot;
     const PsiScale<R> ps = load_scales<R>(ip.sc, cur);
-    DD acc[MAXQ];
+    // reduced quantities: three per component (norm, <h_mu>, <h_en> or the
+    // role's equivalents); a one-field pass serves one component
+    constexpr int NQ = NF == 1 ? 3 : MAXQ;
+    DD acc[NQ];
 #pragma unroll
-    for (int q = 0; q < MAXQ; ++q) acc[q] = DD{0.0, 0.0};
+    for (int q = 0; q < NQ; ++q) acc[q] = DD{0.0, 0.0};
     C v[NF][E];
 
     if constexpr (KIND == XK_FWD || KIND == XK_FULL) {
@@ -899,7 +902,7 @@ __device__ __forceinline__ void xpass_tile(const PassArgs<R>& a, int rows, unsig
         }
         if constexpr (kind_reduces<KIND>()) {
             if (epi_reduces(a)) {
-                reduce_and_finalize<R, MAXQ>(a, ip, acc, reduce_scratch(), tile, ntiles);
+                reduce_and_finalize<R, NQ>(a, ip, acc, reduce_scratch(), tile, ntiles);
             }
         }
     }
