@@ -2725,9 +2725,11 @@ gpe_status tune_handle_t(gpe_handle* h, int workload, double* report) {
     const int rmax = (256 / T) > 0 ? 256 / T : 1;
     int best_r = 0;
     double best_us = 1e30;
-    // down to a quarter of the longest tile: at 128 (16 threads a row) four
-    // rows make 64-thread CTAs, sixteen of which fill an SM's 64 warps
-    for (int r = rmax; r >= 1 && r >= rmax / 4; --r) {
+    // from a quarter of the longest tile up: at 128 (16 threads a row) four
+    // rows make 64-thread CTAs, sixteen of which fill an SM's 64 warps; a
+    // larger tile is kept only when it is 1 % faster, so near-ties go to the
+    // fuller occupancy (whose lead grows when the step starts from a cold L2)
+    for (int r = rmax / 4 > 1 ? rmax / 4 : 1; r <= rmax; ++r) {
         h->xrows = (r == rmax) ? 0 : r;
         double us = 0.0;
         GPE_TRY(time_steps<R>(h, workload, &us));
