@@ -74,6 +74,9 @@ def parse():
     p.add_argument("--persistent-step", default="tuned", choices=["tuned", "on", "strided", "off"],
                    help="complex64 persistent launches (gpe_set_flow): the tuner's choice, one launch per step "
                         "(on), one launch per stage's strided passes (strided), or the per-pass chain (off)")
+    p.add_argument("--oracle-steps", type=int, default=0,
+                   help="also run the FP64 oracle (the checker of the CPU leg) to this many steps and compare "
+                        "both GPU forms with it there (10000: about 14 min on 16 host cores)")
     p.add_argument("--sweep-converge", action="store_true",
                    help="sweep2d: also run every instance to |dmu| < 1e-8 and report the iterations")
     return p.parse_args()
@@ -394,7 +397,7 @@ def run_ours(args):
 
     if not args.quick:
         line["accuracy"] = accuracy(solvers, psi_gs, args.accuracy_steps)
-        line["cpu_baseline"] = cpu_baseline(n, psi_gs, solvers)
+        line["cpu_baseline"] = cpu_baseline(n, psi_gs, solvers, long_steps=args.oracle_steps)
         if world == 1:
             # the reference's own CUDA build (complex128, cuFFT) on this GPU,
             # same loop: the GPU-vs-GPU comparison figure
@@ -439,11 +442,14 @@ def accuracy(solvers, psi_gs, nsteps):
     return out
 
 
-def cpu_baseline(n, psi_gs, solvers=None, budget_s=12.0):
+def cpu_baseline(n, psi_gs, solvers=None, budget_s=12.0, long_steps=0):
     """FP64 oracle port of the reference algorithm on the host cores, timed
     over a bounded sample of the workload: k RK4 steps from the same ground
     state.  The oracle's state after the sample is then the checker for both
-    GPU forms run over the same k steps (psi, E and mu relative errors)."""
+    GPU forms run over the same k steps (psi, E and mu relative errors).
+    long_steps > k: the oracle continues to long_steps steps (untimed, as the
+    checker only) and both GPU forms are compared with it there, with the
+    norm and energy drift of each against its own start."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py as orc
     import fgpe_b200 as gp
@@ -461,6 +467,34 @@ def cpu_baseline(n, psi_gs, solvers=None, budget_s=12.0):
     oo = o.step_real(1, k, want_obs=True)
     dt = time.perf_counter() - t0
     po = o.get_psi(0)
+    long_run = None
+    if solvers and long_steps > k + 1:
+        o0 = orc.OracleSolver(cfg)
+        o0.set_vext(0, trap(cfg))
+        o0.set_psi(0, psi_gs)
+        ostart = o0.observables(0.0)
+        o0.close()
+        o.step_real(k + 1, long_steps - (k + 1))
+        ol = o.observables(long_steps * DT)
+        pl = o.get_psi(0)
+        long_run = {"steps": long_steps,
+                    "oracle_norm_drift": float(ol[0] / ostart[0] - 1),
+                    "oracle_energy_drift": float((ol[2] / ol[0]) / (ostart[2] / ostart[0]) - 1)}
+        for name, s in solvers.items():
+            s.set_psi(0, psi_gs)
+            g0 = s.observables(0.0)
+            done = 0
+            while done < long_steps:
+                m = min(500, long_steps - done)
+                s.step_real(done, m)
+                done += m
+            gl = s.observables(long_steps * DT)
+            pg = s.get_psi(0)
+            long_run[name] = {"psi_rel_l2": float(np.linalg.norm(pg - pl) / np.linalg.norm(pl)),
+                              "E_rel_err": float(abs(gl[2] / gl[0] - ol[2] / ol[0]) / abs(ol[2] / ol[0])),
+                              "mu_rel_err": float(abs(gl[1] / gl[0] - ol[1] / ol[0]) / abs(ol[1] / ol[0])),
+                              "norm_drift": float(gl[0] / g0[0] - 1),
+                              "energy_drift": float((gl[2] / gl[0]) / (g0[2] / g0[0]) - 1)}
     o.close()
     out = {"value": round(k / dt, 4), "unit": "steps/s", "cores": threads, "kind": "port",
            "sample": f"{k + 1} RK4 steps of the same {n}^3 workload from the same ground state in FP64 "
@@ -475,6 +509,8 @@ def cpu_baseline(n, psi_gs, solvers=None, budget_s=12.0):
                          "E_rel_err": float(abs(og[2] / og[0] - oo[2] / oo[0]) / abs(oo[2] / oo[0])),
                          "mu_rel_err": float(abs(og[1] / og[0] - oo[1] / oo[0]) / abs(oo[1] / oo[0])),
                          "norm_rel_err": float(abs(og[0] / oo[0] - 1))}
+        if long_run is not None:
+            par["long_run"] = long_run
         out["parity_vs_port"] = par
     return out
 
