@@ -953,6 +953,12 @@ gpe_status imag_issue(gpe_handle* h, int first, int nsteps) {
             set_rotation<R>(h, a, true);  // src/oneComponentGPSolver.cu:62 alg_calcHpsi
             GPE_TRY(run_chain<R>(h, a, h->nf));
         } else {
+            // Stages 1-3 x-forward transform the stage state they write (the
+            // next stage's input, XK_RKIF); stage 1 keeps its own x-forward
+            // pass, whose prologue applies the renormalisation scale that
+            // stage 4's reduction sets.
+            const bool can_fuse = h->ny > 1 || h->nz > 1;
+            bool w_ready = false;
             for (int s = 1; s <= 4; ++s) {
                 a.epi = EPI_RKI;
                 a.stage = s;
@@ -960,8 +966,11 @@ gpe_status imag_issue(gpe_handle* h, int first, int nsteps) {
                 for (int c = 0; c < 2; ++c) a.pin[c] = (const C*)h->B[c];
                 a.c_re = (s <= 2) ? -0.5 * dt : -1.0 * dt;
                 a.c_im = 0.0;
-                GPE_TRY(run_chain<R>(h, a, h->nf));
+                a.fuse_fwd = (can_fuse && s < 4) ? 1 : 0;
+                GPE_TRY(run_chain<R>(h, a, h->nf, w_ready));
+                w_ready = a.fuse_fwd != 0;
             }
+            a.fuse_fwd = 0;
         }
     }
     return GPE_OK;

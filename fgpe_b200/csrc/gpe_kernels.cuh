@@ -55,9 +55,12 @@ enum SpecOp { SPEC_NONE = 0, SPEC_KIN = 1, SPEC_PX = 2 };
 // the low part) into its own shared-memory slots with asynchronous copies at
 // kernel start, before the wait on the previous pass, so that they are in
 // flight during the inverse transform (complex64, one field).
+// XK_RKIF is XK_RKI (imaginary-time RK4 stage) followed by the forward x
+// transform of the stage state it wrote (stages 1-3: the next stage's
+// x-forward pass, as XK_RKF does in real time).
 enum XKind { XK_FWD = 0, XK_STORE = 1, XK_RK = 2, XK_HB = 3, XK_RKI = 4, XK_AH = 5, XK_FULL = 6, XK_RKO = 7,
-             XK_RKF = 8, XK_ADJ = 9, XK_RKS = 10 };
-constexpr int NXKIND = 11;  // SPEC_PX: BECVPx, src/parallel.cu:283-292
+             XK_RKF = 8, XK_ADJ = 9, XK_RKS = 10, XK_RKIF = 11 };
+constexpr int NXKIND = 12;  // SPEC_PX: BECVPx, src/parallel.cu:283-292
 
 constexpr int MAXQ = 6;       // reduced quantities per launch (3 per component)
 template <typename R>

@@ -546,15 +546,17 @@ __device__ __forceinline__ void epilogue_point(const PassArgs<R>& a, const typen
                     acc[3 * c + 1] = dd_add(acc[3 * c + 1], p.x * h.x + p.y * h.y);
                     acc[3 * c + 2] = dd_add(acc[3 * c + 2], p.x * he.x + p.y * he.y);
                     a.kacc[c][gi] = hmu[c];
-                    a.buf[1][c][gi] = from_d<C>(rk_axpy(p0[c], a.c_re, a.c_im, h));
+                    nv[c] = from_d<C>(rk_axpy(p0[c], a.c_re, a.c_im, h));
+                    a.buf[1][c][gi] = nv[c];
                 } else if (stage < 4) {
                     const double2 k = to_d(in.k[c]);
                     a.kacc[c][gi] = from_d<C>(make_double2(k.x + 2.0 * h.x, k.y + 2.0 * h.y));
-                    a.buf[1][c][gi] = from_d<C>(rk_axpy(p0[c], a.c_re, a.c_im, h));
+                    nv[c] = from_d<C>(rk_axpy(p0[c], a.c_re, a.c_im, h));
+                    a.buf[1][c][gi] = nv[c];
                 } else {
-                    const C nv = from_d<C>(rk_final(p0[c], a.c_re, a.c_im, to_d(in.k[c]), h));
-                    a.buf[0][c][gi] = nv;
-                    const double2 n = to_d(nv);
+                    nv[c] = from_d<C>(rk_final(p0[c], a.c_re, a.c_im, to_d(in.k[c]), h));
+                    a.buf[0][c][gi] = nv[c];
+                    const double2 n = to_d(nv[c]);
                     acc[3 * c + 0] = dd_add(acc[3 * c + 0], n.x * n.x + n.y * n.y);
                 }
             }
@@ -712,6 +714,8 @@ __device__ __forceinline__ void epilogue_dispatch(const PassArgs<R>& a, const ty
     }
     else if constexpr (KIND == XK_HB) GPE_EPI(EPI_HB, true);
     else if constexpr (KIND == XK_RKI) GPE_EPI(EPI_RKI, true);
+    else if constexpr (KIND == XK_RKIF)  // stages 1-3, the new stage state then x-forward transformed
+        epilogue_line<R, NF, EPI_RKI, true, L, E, T, Rr, true, 0, H>(a, hc, ps, v, g0, cur, acc);
     else if constexpr (KIND == XK_ADJ) GPE_EPI(EPI_ADJ, false);
     else if constexpr (KIND == XK_AH) {
         // the apply-H kernel serves both EPI_APPLYH and EPI_OBS
@@ -739,7 +743,7 @@ __device__ __forceinline__ bool epi_reduces(const PassArgs<R>& a) {
 // Kernel roles that may reduce (the others never touch the partials).
 template <int KIND>
 __host__ __device__ constexpr bool kind_reduces() {
-    return KIND == XK_RKO || KIND == XK_HB || KIND == XK_RKI || KIND == XK_AH || KIND == XK_FULL;
+    return KIND == XK_RKO || KIND == XK_HB || KIND == XK_RKI || KIND == XK_RKIF || KIND == XK_AH || KIND == XK_FULL;
 }
 
 // Resident CTAs per SM the launch bounds ask for: complex64 lines of up to 8
@@ -887,7 +891,7 @@ __device__ __forceinline__ void xpass_tile(const PassArgs<R>& a, int rows, unsig
         } else {
             if (valid) epilogue_dispatch<R, NF, KIND, L, E, T, RinF, H>(a, hc, ps, v, g0, cur, acc);
         }
-        if constexpr (KIND == XK_RKF || KIND == XK_RKS) {
+        if constexpr (KIND == XK_RKF || KIND == XK_RKS || KIND == XK_RKIF) {
             // next stage's x-forward pass on the state just written (in place on w)
 #pragma unroll
             for (int f = 0; f < NF; ++f) line_fft_fwd<L>(v[f], addr, a.tw, t);
@@ -1291,6 +1295,7 @@ cudaError_t launch_xpass(const PassArgs<R>& a, int rows, size_t smem, cudaStream
     int kind = xkind_of(a.mode, a.epi);
     if (kind == XK_RK && a.want_obs && a.stage == 4) kind = XK_RKO;
     else if (kind == XK_RK && a.fuse_fwd) kind = XK_RKF;
+    else if (kind == XK_RKI && a.fuse_fwd) kind = XK_RKIF;
     if constexpr (NF == 1 && sizeof(R) == 4 && H::builtin) {
         if (kind == XK_RKF && a.xstage) {  // staged epilogue inputs: exchange rows + the staging slots
             const int threads = rows * Plan<L>::T;
@@ -1311,6 +1316,7 @@ cudaError_t launch_xpass(const PassArgs<R>& a, int rows, size_t smem, cudaStream
         case XK_RKF: return launch_xpass_kind<R, L, NF, XK_RKF, H>(a, rows, smem, st);
         case XK_HB: return launch_xpass_kind<R, L, NF, XK_HB, H>(a, rows, smem, st);
         case XK_RKI: return launch_xpass_kind<R, L, NF, XK_RKI, H>(a, rows, smem, st);
+        case XK_RKIF: return launch_xpass_kind<R, L, NF, XK_RKIF, H>(a, rows, smem, st);
         case XK_AH: return launch_xpass_kind<R, L, NF, XK_AH, H>(a, rows, smem, st);
         default: return launch_xpass_kind<R, L, NF, XK_FULL, H>(a, rows, smem, st);
     }

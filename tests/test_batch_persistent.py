@@ -119,10 +119,12 @@ def test_persistent_launches_four_kernels_per_iteration(gpu):
         b.step_imag(3)
         grouped = b.launches - l2
     # per call one iteration-counter reset per group; per iteration 4 stage
-    # kernels, or 3 passes x 4 stages for all groups, or that per group
+    # kernels, or 3 passes x 4 stages for all groups, or per group the
+    # x-forward of stage 1 and 2 passes a stage (stages 1-3 fuse the next
+    # stage's x-forward into their x-inverse pass)
     assert per_stage == len(cfgs) + 4 * 3
     assert grouped == len(cfgs) + 12 * 3
-    assert per_group == len(cfgs) + 12 * 3 * len(cfgs)
+    assert per_group == len(cfgs) + (1 + 2 * 4) * 3 * len(cfgs)
 
 
 def test_persistent_rk4_convergence_stops_each_instance(gpu):
