@@ -60,6 +60,20 @@ def test_host_only_entry_points_work_without_gpu():
     assert L.gpe_create(ctypes.byref(bad), ctypes.byref(h)) == 2  # no FFT plan for 14
 
 
+def test_launch_form_entry_points_reject_bad_arguments_without_gpu():
+    """The persistent-launch and x-staging switches validate their arguments
+    on the host before any device work (null handle, mode out of range)."""
+    import fgpe_b200 as g
+    L = g.lib()
+    st = ctypes.c_int(-1)
+    assert L.gpe_set_flow(None, 1, 0) == 1
+    assert L.gpe_flow_status(None, ctypes.byref(st)) == 1
+    assert L.gpe_flow_active(None) == 0
+    assert L.gpe_set_x_staging(None, 1) == 1
+    assert L.gpe_x_staging(None) == 0
+    assert b"null handle" in L.gpe_last_error_string()
+
+
 def test_config_struct_layout():
     import fgpe_b200 as g
     # int abi, nx, ny, nz, dim; pad; 3+3 doubles; 4 ints; 32 doubles; dt, beta, npart[2], eps; 8 ints
