@@ -2829,6 +2829,17 @@ gpe_status tune_handle_t(gpe_handle* h, int workload, double* report) {
         }
         GPE_CUDA(cudaStreamSynchronize(h->st));
     }
+    // the choices were made pass by pass and step by step; keep them only if
+    // together they beat the default variants (small grids are noisy)
+    if (!(tuned_us < def_us)) {
+        for (int ax = 0; ax < 3; ++ax)
+            for (int m = 0; m < 3; ++m) h->svar[ax][m] = 0;
+        h->xrows = 0;
+        h->yz = 0;
+        h->flow = 0;
+        h->xstage = 0;
+        tuned_us = def_us;
+    }
     if (report) {
         report[0] = def_us;
         report[1] = tuned_us;

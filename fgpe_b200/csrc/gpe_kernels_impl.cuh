@@ -761,12 +761,22 @@ __host__ __device__ constexpr int pass_min_blocks() {
 // memory: one padded exchange row per line (rows * xpad(L) elements).
 // Roles with the FP64 reductions hold more live values: one CTA fewer.  The
 // one-field real-time RK roles fit 64 registers: one CTA more.
+// The one-field heavy-ball and apply-H roles (both precisions) and the
+// complex64 observables role carry three reduced sums and fit the
+// non-reducing budget without spills for lines of 8 values (-Xptxas -v:
+// 80 registers complex64, 128 complex128), so they keep the CTA.
+template <typename R, int L, int NF, int KIND>
+__host__ __device__ constexpr bool xpass_light_reduce() {
+    return NF == 1 && Plan<L>::E == 8 &&
+           (KIND == XK_HB || KIND == XK_AH || (KIND == XK_RKO && sizeof(R) == 4));
+}
 template <typename R, int L, int NF, int KIND>
 __host__ __device__ constexpr int xpass_min_blocks() {
     return (NF == 1 && (KIND == XK_RKF || KIND == XK_RK || KIND == XK_RKS) && pass_min_blocks<R, L, NF>() == 3)
                ? 4
-               : (kind_reduces<KIND>() && pass_min_blocks<R, L, NF>() > 1 ? pass_min_blocks<R, L, NF>() - 1
-                                                                           : pass_min_blocks<R, L, NF>());
+               : (kind_reduces<KIND>() && pass_min_blocks<R, L, NF>() > 1 && !xpass_light_reduce<R, L, NF, KIND>()
+                      ? pass_min_blocks<R, L, NF>() - 1
+                      : pass_min_blocks<R, L, NF>());
 }
 
 // Warms L2 with a tile's real-time RK epilogue inputs (V, the stage state
